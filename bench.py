@@ -1,0 +1,324 @@
+#!/usr/bin/env python
+"""RS(10,4) Encode on B200: device-resident throughput, end-to-end over PCIe,
+HBM roofline, and the CPU reference timed on the same host.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one "step"): Encode of one RS(10,4) stripe of 10 x 64 MiB uniform
+random data shards into 4 x 64 MiB parity shards (the configuration the
+headline metric is quoted on).  Inputs (640 MiB) are larger than the 126 MB
+L2, so no flush is needed between steps.  Under torchrun every rank encodes
+its own stripe on its own GPU (independent stripes: weak scaling, no
+data-path collective); the timed region is bracketed by barriers and the
+max over ranks is reported.
+
+value      = data GB/s (k * shard bytes / step time), device-resident, kernel
+             launches back to back on one stream, CUDA-event timed.
+e2e        = same metric through the C-ABI host-buffer entry point
+             (rsgpu_encode_host): H2D of the data shards from pinned memory,
+             encode, D2H of the parity, pipelined inside the call.
+roofline   = (k+p) * shard bytes per launch / average launch time, against
+             the measured HBM copy bandwidth (MEASURED_PEAKS.json).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+K_DATA, P_PARITY, SHARD = 10, 4, 64 << 20
+METRIC = "RS(10,4) encode data GB/s (10 x 64 MiB shards)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=10.0,
+                    help="bounded CPU-baseline sample length")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
+    ap.add_argument("--shard-mib", type=int, default=SHARD >> 20,
+                    help="shard size; the headline workload is 64 MiB")
+    ap.add_argument("--variant", type=int, default=-1,
+                    help="force one GF(2^8) kernel variant instead of autotuning (profiling runs)")
+    return ap.parse_args()
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per launch from the committed ncu summary of this workload, if any."""
+    p = os.path.join(ROOT, "profiles", "gf8_encode_rs10x4_64MiB.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f).get("dram_bytes_per_launch")
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+            time.sleep(0.3)
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == 7:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.2)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[3 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def cpu_reference(seconds, threads, shard=SHARD, max_steps=None):
+    """The reference's SIMD algorithm (GFNI/AVX2 restated in oracle_simd.c) on all host threads."""
+    import oracle as O
+    rng = np.random.default_rng(0)
+    k, p = K_DATA, P_PARITY
+    _, m = O.build_matrix("default", k, k + p)
+    rows = m[k:]
+    data = [rng.integers(0, 256, shard, dtype=np.uint8) for _ in range(k)]
+    par = [np.empty(shard, np.uint8) for _ in range(p)]
+    O.code_some_shards_fast(rows, data, par, True, threads)  # warm
+    n, t0 = 0, time.perf_counter()
+    while True:
+        O.code_some_shards_fast(rows, data, par, True, threads)
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or (max_steps and n >= max_steps):
+            break
+    isa = {2: "avx512+gfni", 1: "avx2", 0: "scalar"}[O.simd_level()]
+    return k * shard * n / el / 1e9, n, el, isa
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup(args)
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    # each step: one full RS(10,4) x 64 MiB encode on the host cores
+    for _ in range(max(args.warmup, 0)):
+        cpu_reference(0.0, threads, max_steps=1)
+    gbs, n, el, isa = cpu_reference(1e9, threads, max_steps=max(args.steps, 1))
+    out = {
+        "impl": "reference", "metric": METRIC, "value": round(gbs, 3), "unit": "GB/s",
+        "n_gpus": args.gpus, "steps": n, "warmup": args.warmup, "ms_per_step": round(el / n * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": "RS(10,4) encode, 10 x 64 MiB uint8 uniform-random data shards",
+                   "k": K_DATA, "p": P_PARITY, "shard_bytes": SHARD, "l2": "inputs > L2"},
+        "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+                         "sample": "%d full encodes of the workload; %s kernels restated from the reference "
+                                   "(Go toolchain absent, reference not runnable)" % (n, isa)},
+        "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+    return 0
+
+
+def run_e2e(args, enc, lib, shards, S, stream, dev, world, barrier):
+    """Encode through the host-buffer C-ABI entry point; every step moves the
+    data shards H2D from pinned memory and the parity D2H."""
+    import torch
+    import torch.distributed as dist
+    import reedsolomon_b200 as rs
+    k, p = K_DATA, P_PARITY
+    hs = [torch.empty(S, dtype=torch.uint8, pin_memory=True) for _ in range(k + p)]
+    for i in range(k):
+        hs[i].copy_(shards[i])
+    hptrs = rs._lib.ptr_array([h.data_ptr() for h in hs])
+    e2e_steps = max(3, min(args.steps, 10))
+    for _ in range(2):
+        rs.encoder.check(lib.rsgpu_encode_host(enc._h, hptrs, S))
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        rs.encoder.check(lib.rsgpu_encode_host(enc._h, hptrs, S))
+    e1.record(stream)
+    barrier()
+    ems = e0.elapsed_time(e1)
+    if world > 1:
+        tt = torch.tensor([ems], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ems = float(tt.item())
+    for i in range(k, k + p):
+        assert torch.equal(hs[i].to(dev), shards[i]), "host-path parity differs from device path"
+    return world * k * S / (ems / e2e_steps / 1e3) / 1e9
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    import reedsolomon_b200 as rs
+
+    dev = torch.device("cuda", local)
+    k, p, S = K_DATA, P_PARITY, args.shard_mib << 20
+    g = torch.Generator(device=dev).manual_seed(1000 + rank)
+    shards = [torch.randint(0, 256, (S,), dtype=torch.uint8, device=dev, generator=g) for _ in range(k)]
+    shards += [torch.empty(S, dtype=torch.uint8, device=dev) for _ in range(p)]
+    enc = rs.New(k, p, rs.WithGPU(local))
+    lib = rs.lib()
+    ptrs = rs._lib.ptr_array([s.data_ptr() for s in shards])
+    stream = torch.cuda.current_stream(dev)
+    enc.ctx.bind_current_stream()
+
+    # autotune the GF(2^8) kernel variant for this geometry (times each variant
+    # on scratch buffers of the same size; the choice is kept for this size bucket)
+    import ctypes
+    tune_ms = (ctypes.c_float * lib.rsgpu_num_variants())()
+    best = ctypes.c_int()
+    if args.variant >= 0:
+        rs.encoder.check(lib.rsgpu_force_variant(args.variant))
+        tuning = {"forced": args.variant}
+    else:
+        rs.encoder.check(lib.rsgpu_autotune_gf8(enc.ctx.handle, k, p, S, 0, 5, tune_ms, ctypes.byref(best)))
+        tuning = {"variant_ms": [round(x, 4) for x in tune_ms], "chosen": best.value}
+
+    def step():
+        rc = lib.rsgpu_encode_async(enc._h, ptrs, S)
+        if rc:
+            rs.encoder.check(rc)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    # correctness guard on the measured buffers
+    assert enc.Verify(shards), "encode produced parity that does not verify"
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    with ClockSampler(local) as clk:
+        barrier()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(args.steps):
+            step()
+        t1.record(stream)
+        barrier()
+    ms = t0.elapsed_time(t1)
+    if world > 1:
+        tt = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    ms_step = ms / args.steps
+    value = world * k * S / (ms_step / 1e3) / 1e9
+    peak, peak_kind = peaks()
+    achieved = (k + p) * S / (ms_step / 1e3) / 1e9
+
+    # end to end: pinned host buffers through rsgpu_encode_host
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, enc, lib, shards, S, stream, dev, world, barrier)
+
+    out = None
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic",
+            "config": {"workload": "RS(10,4) encode, 10 x 64 MiB uint8 uniform-random data shards per GPU",
+                       "k": k, "p": p, "shard_bytes": S, "l2": "inputs (%d MiB) > L2, no flush" % (k * S >> 20),
+                       "parallelism": "independent stripes per GPU"},
+            "reference_convention_GBps": round(world * (k + p) * S / (ms_step / 1e3) / 1e9, 3),
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": profile_traffic(),
+                         "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
+                         "algorithmic_bytes_per_launch": (k + p) * S},
+            "e2e": None if e2e is None else {
+                "value": round(e2e, 3), "unit": "GB/s", "h2d_bytes_per_step": k * S,
+                "d2h_bytes_per_step": p * S, "path": "rsgpu_encode_host, pinned host buffers"},
+            "gpu_launches": args.steps,
+            "autotune": tuning,
+            "clocks": clk.summary(),
+        }
+        if not args.no_cpu_baseline:
+            threads = os.cpu_count() or 1
+            gbs, n, el, isa = cpu_reference(args.cpu_seconds, threads, shard=16 << 20)
+            out["cpu_baseline"] = {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+                                   "sample": "RS(10,4) x 16 MiB encodes for %.1f s (%d encodes), %s kernels "
+                                             "restated from the reference" % (el, n, isa)}
+        print(json.dumps(out))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    sys.path.insert(0, ROOT)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,192 @@
+/*
+ * rsgpu.h -- C-ABI of the B200 erasure-coding engine (librsgpu.so).
+ *
+ * Drop-in boundary for klauspost/reedsolomon's hot path.  Each entry point
+ * names the reference interface it replaces (paths inside the reference
+ * project).  All functions are plain C: pointers and sizes only.
+ *
+ * Memory model
+ *   - "shards" arguments of the device entry points are host arrays of DEVICE
+ *     pointers (one per shard), like the reference's [][]byte.
+ *   - *_host entry points take host arrays of HOST pointers; the library moves
+ *     the bytes over PCIe (pinned host memory gives full PCIe bandwidth).
+ *   - The caller owns every shard buffer.  A missing output shard passed as
+ *     NULL is allocated by the library (rsgpu_free releases it), mirroring the
+ *     reference's AllocAligned of missing shards (reedsolomon.go:1747-1751).
+ *   - A missing shard is marked by present[i] == 0 (the reference uses a
+ *     zero-length slice, reedsolomon.go:1680-1696).
+ *   - Calls are synchronous with respect to the host unless named *_async:
+ *     they enqueue on the context stream and wait, keeping the reference's
+ *     blocking semantics.
+ *
+ * Status codes map 1:1 onto the reference's sentinel errors.
+ */
+#ifndef RSGPU_H
+#define RSGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define RS_OK 0
+#define RS_ERR_TOO_FEW_SHARDS -1        /* ErrTooFewShards      reedsolomon.go:678 */
+#define RS_ERR_SHARD_NO_DATA -2         /* ErrShardNoData       reedsolomon.go:1391 */
+#define RS_ERR_SHARD_SIZE -3            /* ErrShardSize         reedsolomon.go:1395 */
+#define RS_ERR_INVALID_SHARD_SIZE -4    /* ErrInvalidShardSize  reedsolomon.go:1399 */
+#define RS_ERR_INV_SHARD_NUM -5         /* ErrInvShardNum       reedsolomon.go:216 */
+#define RS_ERR_MAX_SHARD_NUM -6         /* ErrMaxShardNum       reedsolomon.go:221 */
+#define RS_ERR_NOT_SUPPORTED -7         /* ErrNotSupported      reedsolomon.go:224 */
+#define RS_ERR_INVALID_INPUT -8         /* ErrInvalidInput      reedsolomon.go:760 */
+#define RS_ERR_RECONSTRUCT_REQUIRED -9  /* ErrReconstructRequired reedsolomon.go:1862 */
+#define RS_ERR_SINGULAR -10             /* errSingular          matrix.go:184 */
+#define RS_ERR_NOT_SQUARE -11           /* errNotSquare         matrix.go:187 */
+#define RS_ERR_CUDA -100                /* a CUDA call failed (see rsgpu_last_error) */
+#define RS_ERR_NOMEM -101               /* device or pinned allocation failed */
+#define RS_ERR_TIMEOUT -102             /* a bounded device wait expired */
+#define RS_ERR_NO_DEVICE -103           /* encoder has no device context */
+
+/* ---- codecs and matrix kinds --------------------------------------------- */
+#define RS_CODEC_CLASSIC 0   /* reedSolomon (reedsolomon.go:170) */
+#define RS_CODEC_LEOPARD16 1 /* leopardFF16 (leopard.go:36) */
+#define RS_CODEC_LEOPARD8 2  /* leopardFF8  (leopard8.go:22) */
+
+#define RS_MATRIX_DEFAULT 0  /* buildMatrix          reedsolomon.go:232 */
+#define RS_MATRIX_CAUCHY 1   /* WithCauchyMatrix     options.go:249 */
+#define RS_MATRIX_PAR1 2     /* WithPAR1Matrix       options.go:237 */
+#define RS_MATRIX_JERASURE 3 /* WithJerasureMatrix   options.go:225 */
+
+#define RS_LEOPARD_AS_NEEDED 0 /* leopardAsNeeded options.go:68 */
+#define RS_LEOPARD_GF16 1      /* WithLeopardGF16 options.go:283 */
+#define RS_LEOPARD_ALWAYS 2    /* WithLeopardGF   options.go:297 */
+
+typedef struct rsgpu_ctx rsgpu_ctx;
+typedef struct rsgpu_encoder rsgpu_encoder;
+
+/* Functional options of New (options.go:13-44).  CPU-tuning options
+ * (goroutines, split sizes, ISA toggles, stream options) have no meaning on
+ * the GPU and are absent. */
+typedef struct rsgpu_options {
+    int matrix_kind;             /* RS_MATRIX_*; options.go:225-258 */
+    int fast_one_parity;         /* WithFastOneParityMatrix options.go:260 */
+    int leopard;                 /* RS_LEOPARD_*; WithLeopardGF16 / WithLeopardGF */
+    int inversion_cache;         /* WithInversionCache options.go:152 (default 1) */
+    const uint8_t *custom_matrix;/* WithCustomMatrix options.go:272: rows x cols, row-major, or NULL */
+    int custom_rows, custom_cols;
+} rsgpu_options;
+
+/* ---- context: device, stream, scratch ------------------------------------ */
+/* Creates a context on `device` with its own non-blocking stream. */
+int rsgpu_ctx_create(int device, rsgpu_ctx **out);
+int rsgpu_ctx_destroy(rsgpu_ctx *ctx);
+/* Run on an external cudaStream_t, used verbatim (NULL is the legacy default
+ * stream); rsgpu_ctx_reset_stream returns to the context's own stream. */
+int rsgpu_ctx_set_stream(rsgpu_ctx *ctx, void *cuda_stream);
+int rsgpu_ctx_reset_stream(rsgpu_ctx *ctx);
+void *rsgpu_ctx_stream(rsgpu_ctx *ctx);
+int rsgpu_ctx_synchronize(rsgpu_ctx *ctx);
+/* Human-readable name of a status code, and the last error text of this thread. */
+const char *rsgpu_status_string(int status);
+const char *rsgpu_last_error(void);
+
+/* ---- memory helpers ------------------------------------------------------- */
+/* AllocAligned (unsafe.go:19-43): n shards of `each` bytes in one device
+ * allocation, each starting on a 64-byte boundary; out[0] owns the block. */
+int rsgpu_alloc_shards(rsgpu_ctx *ctx, int n, size_t each, uint8_t **out);
+int rsgpu_free(rsgpu_ctx *ctx, void *device_ptr);
+int rsgpu_host_alloc(size_t bytes, void **out); /* pinned host memory */
+int rsgpu_host_free(void *p);
+
+/* ---- encoder (Encoder / Extensions interfaces, reedsolomon.go:25-165) ----- */
+void rsgpu_options_init(rsgpu_options *opts);
+/* New (reedsolomon.go:425-601).  ctx may be NULL for a host-only encoder that
+ * can plan (rsgpu_decode_plan) but not run device work. */
+int rsgpu_encoder_new(rsgpu_ctx *ctx, int data_shards, int parity_shards, const rsgpu_options *opts,
+                      rsgpu_encoder **out);
+int rsgpu_encoder_free(rsgpu_encoder *enc);
+/* DataShards / ParityShards / TotalShards / ShardSizeMultiple (reedsolomon.go:141-165) */
+int rsgpu_encoder_info(const rsgpu_encoder *enc, int *data_shards, int *parity_shards,
+                       int *shard_size_multiple, int *codec);
+/* The (k+p) x k encoding matrix of a classic encoder (reedSolomon.m). */
+int rsgpu_encoder_matrix(const rsgpu_encoder *enc, uint8_t *out);
+
+/* Encode (reedsolomon.go:686-702; leopard.go:139; leopard8.go:128) */
+int rsgpu_encode(rsgpu_encoder *enc, uint8_t *const *shards, size_t shard_size);
+/* EncodeIdx (reedsolomon.go:708-757): parity[o] ^= M[k+o][idx] * data */
+int rsgpu_encode_idx(rsgpu_encoder *enc, const uint8_t *data_shard, int idx, uint8_t *const *parity,
+                     size_t shard_size);
+/* Verify (reedsolomon.go:857-871; leopard.go:393-419) */
+int rsgpu_verify(rsgpu_encoder *enc, uint8_t *const *shards, size_t shard_size, int *ok);
+/* Reconstruct / ReconstructData / ReconstructSome (reedsolomon.go:1446,1634,1655;
+ * leopard.go:378-391).  required has n_required entries (k or k+p).
+ * written (optional, k+p entries) reports which shards were filled. */
+int rsgpu_reconstruct(rsgpu_encoder *enc, uint8_t **shards, const uint8_t *present,
+                      size_t shard_size, uint8_t *written);
+int rsgpu_reconstruct_data(rsgpu_encoder *enc, uint8_t **shards, const uint8_t *present,
+                           size_t shard_size, uint8_t *written);
+int rsgpu_reconstruct_some(rsgpu_encoder *enc, uint8_t **shards, const uint8_t *present,
+                           const uint8_t *required, int n_required, size_t shard_size,
+                           uint8_t *written);
+
+/* Asynchronous variants: enqueue on the context stream and return without
+ * waiting (the caller orders later work on that stream or synchronises).
+ * Missing reconstruct outputs must be preallocated (no NULL entries). */
+int rsgpu_encode_async(rsgpu_encoder *enc, uint8_t *const *shards, size_t shard_size);
+int rsgpu_reconstruct_async(rsgpu_encoder *enc, uint8_t *const *shards, const uint8_t *present,
+                            size_t shard_size, int data_only);
+
+/* Host-buffer variants: shards are HOST pointers; H2D/D2H happen inside,
+ * pipelined in column chunks over two copy directions and the compute stream. */
+int rsgpu_encode_host(rsgpu_encoder *enc, uint8_t *const *host_shards, size_t shard_size);
+int rsgpu_reconstruct_host(rsgpu_encoder *enc, uint8_t **host_shards, const uint8_t *present,
+                           size_t shard_size, int data_only, uint8_t *written);
+
+/* Decode planning without device work: the rows codeSomeShards receives in
+ * reconstruct (reedsolomon.go:1710-1779).  rows_out[n_out x k], out_idx[n_out],
+ * in_idx[k] = the first k present shards.  n_out == 0: nothing to do. */
+int rsgpu_decode_plan(rsgpu_encoder *enc, const uint8_t *present, int data_only,
+                      const uint8_t *required, int n_required, uint8_t *rows_out, int *out_idx,
+                      int *n_out, int *in_idx);
+
+/* ---- kernel seam (galois_gen_switch_amd64.go:29-44 fn pointers) ---------- */
+/* codeSomeShards (reedsolomon.go:882-975): out[o][start:stop] (^)= sum_i
+ * rows[o*n_in+i] * in[i][start:stop]; clear=1 overwrites, 0 accumulates. */
+int rsgpu_code_some_shards(rsgpu_ctx *ctx, const uint8_t *rows, int n_in, int n_out,
+                           const uint8_t *const *in, uint8_t *const *out, size_t start, size_t stop,
+                           int clear);
+/* checkSomeShards (reedsolomon.go:1373-1387) fused: *ok = all(rows*in == to_check) */
+int rsgpu_check_some_shards(rsgpu_ctx *ctx, const uint8_t *rows, int n_in, int n_out,
+                            const uint8_t *const *in, const uint8_t *const *to_check,
+                            size_t nbytes, int *ok);
+/* galMulSlice / galMulSliceXor (galois_amd64.go:49-159; mulslice.go:29-38) */
+int rsgpu_gal_mul_slice(rsgpu_ctx *ctx, uint8_t c, const uint8_t *in, uint8_t *out, size_t n,
+                        int xor_into);
+/* sliceXor (galois_amd64.go:162-203): out ^= in */
+int rsgpu_slice_xor(rsgpu_ctx *ctx, const uint8_t *in, uint8_t *out, size_t n);
+
+/* ---- autotuner (no counterpart in the reference: CPU dispatch there is by
+ * cpuid, galois_gen_switch_amd64.go:29-44) -------------------------------- */
+/* Times every GF(2^8) kernel variant on scratch buffers of the given geometry
+ * (n_in <= 32, n_out <= 16) and records the fastest for that geometry and
+ * size bucket; ms_out (optional) receives the per-variant milliseconds. */
+int rsgpu_autotune_gf8(rsgpu_ctx *ctx, int n_in, int n_out, size_t nbytes, int mode, int reps,
+                       float *ms_out, int *best_out);
+/* Force one variant for every launch (-1 restores the tuned choice). */
+int rsgpu_force_variant(int variant);
+int rsgpu_num_variants(void);
+
+/* ---- host algebra (CPU only, no device needed) --------------------------- */
+/* buildMatrix* (reedsolomon.go:232-413): (total x k) row-major */
+int rsgpu_build_matrix(int matrix_kind, int data_shards, int total_shards, uint8_t *out);
+/* matrix.Invert (matrix.go:192-207) */
+int rsgpu_invert_matrix(const uint8_t *m, int n, uint8_t *out);
+/* galMultiply (galois.go:852) */
+uint8_t rsgpu_gal_mul(uint8_t a, uint8_t b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RSGPU_H */

@@ -1,0 +1,105 @@
+"""ctypes binding of librsgpu.so (the C-ABI declared in include/rsgpu.h).
+
+The library is built in-tree by reedsolomon_b200.build; importing this module
+never falls back to anything else: a missing or unloadable library raises.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "librsgpu.so")
+
+c_u8p = ctypes.POINTER(ctypes.c_uint8)
+c_voidp = ctypes.c_void_p
+c_size = ctypes.c_size_t
+c_int = ctypes.c_int
+c_intp = ctypes.POINTER(ctypes.c_int)
+
+
+class RsOptions(ctypes.Structure):
+    _fields_ = [
+        ("matrix_kind", c_int),
+        ("fast_one_parity", c_int),
+        ("leopard", c_int),
+        ("inversion_cache", c_int),
+        ("custom_matrix", c_voidp),
+        ("custom_rows", c_int),
+        ("custom_cols", c_int),
+    ]
+
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "rsgpu_ctx_create": (c_int, [c_int, ctypes.POINTER(c_voidp)]),
+    "rsgpu_ctx_destroy": (c_int, [c_voidp]),
+    "rsgpu_ctx_set_stream": (c_int, [c_voidp, c_voidp]),
+    "rsgpu_ctx_reset_stream": (c_int, [c_voidp]),
+    "rsgpu_ctx_stream": (c_voidp, [c_voidp]),
+    "rsgpu_ctx_synchronize": (c_int, [c_voidp]),
+    "rsgpu_status_string": (ctypes.c_char_p, [c_int]),
+    "rsgpu_last_error": (ctypes.c_char_p, []),
+    "rsgpu_alloc_shards": (c_int, [c_voidp, c_int, c_size, c_voidp]),
+    "rsgpu_free": (c_int, [c_voidp, c_voidp]),
+    "rsgpu_host_alloc": (c_int, [c_size, ctypes.POINTER(c_voidp)]),
+    "rsgpu_host_free": (c_int, [c_voidp]),
+    "rsgpu_options_init": (None, [ctypes.POINTER(RsOptions)]),
+    "rsgpu_encoder_new": (c_int, [c_voidp, c_int, c_int, ctypes.POINTER(RsOptions), ctypes.POINTER(c_voidp)]),
+    "rsgpu_encoder_free": (c_int, [c_voidp]),
+    "rsgpu_encoder_info": (c_int, [c_voidp, c_intp, c_intp, c_intp, c_intp]),
+    "rsgpu_encoder_matrix": (c_int, [c_voidp, c_voidp]),
+    "rsgpu_encode": (c_int, [c_voidp, c_voidp, c_size]),
+    "rsgpu_encode_idx": (c_int, [c_voidp, c_voidp, c_int, c_voidp, c_size]),
+    "rsgpu_verify": (c_int, [c_voidp, c_voidp, c_size, c_intp]),
+    "rsgpu_reconstruct": (c_int, [c_voidp, c_voidp, c_voidp, c_size, c_voidp]),
+    "rsgpu_reconstruct_data": (c_int, [c_voidp, c_voidp, c_voidp, c_size, c_voidp]),
+    "rsgpu_reconstruct_some": (c_int, [c_voidp, c_voidp, c_voidp, c_voidp, c_int, c_size, c_voidp]),
+    "rsgpu_encode_async": (c_int, [c_voidp, c_voidp, c_size]),
+    "rsgpu_reconstruct_async": (c_int, [c_voidp, c_voidp, c_voidp, c_size, c_int]),
+    "rsgpu_encode_host": (c_int, [c_voidp, c_voidp, c_size]),
+    "rsgpu_reconstruct_host": (c_int, [c_voidp, c_voidp, c_voidp, c_size, c_int, c_voidp]),
+    "rsgpu_decode_plan": (c_int, [c_voidp, c_voidp, c_int, c_voidp, c_int, c_voidp, c_voidp, c_intp, c_voidp]),
+    "rsgpu_code_some_shards": (c_int, [c_voidp, c_voidp, c_int, c_int, c_voidp, c_voidp, c_size, c_size, c_int]),
+    "rsgpu_check_some_shards": (c_int, [c_voidp, c_voidp, c_int, c_int, c_voidp, c_voidp, c_size, c_intp]),
+    "rsgpu_gal_mul_slice": (c_int, [c_voidp, ctypes.c_uint8, c_voidp, c_voidp, c_size, c_int]),
+    "rsgpu_slice_xor": (c_int, [c_voidp, c_voidp, c_voidp, c_size]),
+    "rsgpu_autotune_gf8": (c_int, [c_voidp, c_int, c_int, c_size, c_int, c_int, c_voidp, c_intp]),
+    "rsgpu_force_variant": (c_int, [c_int]),
+    "rsgpu_num_variants": (c_int, []),
+    "rsgpu_build_matrix": (c_int, [c_int, c_int, c_int, c_voidp]),
+    "rsgpu_invert_matrix": (c_int, [c_voidp, c_int, c_voidp]),
+    "rsgpu_gal_mul": (ctypes.c_uint8, [ctypes.c_uint8, ctypes.c_uint8]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load librsgpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                "librsgpu.so is missing at %s; build it with `python -m reedsolomon_b200.build`" % LIB_PATH)
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            if hasattr(L, name):
+                f = getattr(L, name)
+                f.restype = res
+                f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def ptr_array(ptrs):
+    """Host array of device (or host) pointers, as the C-ABI's uint8_t** arguments."""
+    arr = (c_voidp * max(1, len(ptrs)))()
+    for i, p in enumerate(ptrs):
+        arr[i] = p if p else None
+    return arr
+
+
+def u8_array(vals):
+    arr = (ctypes.c_uint8 * max(1, len(vals)))()
+    for i, v in enumerate(vals):
+        arr[i] = int(v)
+    return arr

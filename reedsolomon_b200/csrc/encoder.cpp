@@ -1,0 +1,662 @@
+// encoder.cpp -- C-ABI runtime: contexts, the classic codec and the kernel seam.
+//
+// Mirrors the reference's Encoder/Extensions behaviour (reedsolomon.go) on
+// device-resident shards: argument checks and error codes follow the Go
+// methods, the decode matrix comes from the host inversion tree, and every
+// contraction is one launch_gf8_matmul on the context stream.
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "rsgpu_internal.h"
+
+namespace rsgpu {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+int cuda_status(cudaError_t e, const char *what) {
+    char buf[512];
+    snprintf(buf, sizeof buf, "%s: %s (%d)", what, cudaGetErrorString(e), (int)e);
+    set_error(buf);
+    if (e == cudaErrorMemoryAllocation) return RS_ERR_NOMEM;
+    return RS_ERR_CUDA;
+}
+
+int DeviceBuffer::ensure(size_t want) {
+    if (want <= bytes) return RS_OK;
+    release();
+    void *p = nullptr;
+    RS_CUDA(cudaMalloc(&p, want));
+    ptr = (uint8_t *)p;
+    bytes = want;
+    return RS_OK;
+}
+
+void DeviceBuffer::release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+// codeSomeShards's "clear" flag selects overwrite vs accumulate.
+static int run_matmul(rsgpu_ctx *ctx, const uint8_t *rows, int n_in, int n_out,
+                      const uint8_t *const *in, uint8_t *const *out, size_t nbytes, int mode) {
+    RS_CUDA(launch_gf8_matmul(ctx->stream, ctx->info, rows, n_in, n_out, in, out, nbytes, mode,
+                              ctx->d_flag));
+    return RS_OK;
+}
+
+static int sync(rsgpu_ctx *ctx) {
+    RS_CUDA(cudaStreamSynchronize(ctx->stream));
+    return RS_OK;
+}
+
+// Fused checkSomeShards: the flag is cleared, the verify launch sets it on a
+// mismatch.  Inputs beyond one launch tile are summed into scratch first.
+static int check_shards(rsgpu_ctx *ctx, const uint8_t *rows, int n_in, int n_out,
+                        const uint8_t *const *in, const uint8_t *const *to_check, size_t nbytes,
+                        int *ok) {
+    RS_CUDA(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
+    if (n_in <= kMaxIn) {
+        int rc = run_matmul(ctx, rows, n_in, n_out, in, const_cast<uint8_t *const *>(to_check),
+                            nbytes, kModeVerify);
+        if (rc) return rc;
+    } else {
+        size_t pitch = (nbytes + 255) & ~(size_t)255;
+        int rc = ctx->scratch.ensure(pitch * (size_t)n_out);
+        if (rc) return rc;
+        std::vector<uint8_t *> tmp(n_out);
+        for (int o = 0; o < n_out; o++) tmp[o] = ctx->scratch.ptr + pitch * o;
+        rc = run_matmul(ctx, rows, n_in, n_out, in, tmp.data(), nbytes, kModeWrite);
+        if (rc) return rc;
+        const uint8_t one = 1;
+        for (int o = 0; o < n_out; o++) {
+            const uint8_t *src = tmp[o];
+            uint8_t *chk = const_cast<uint8_t *>(to_check[o]);
+            rc = run_matmul(ctx, &one, 1, 1, &src, &chk, nbytes, kModeVerify);
+            if (rc) return rc;
+        }
+    }
+    RS_CUDA(cudaMemcpyAsync(ctx->h_flag, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    int rc = sync(ctx);
+    if (rc) return rc;
+    *ok = (*ctx->h_flag == 0);
+    return RS_OK;
+}
+
+// reedsolomon.go:1670-1781: select the first k present shards, fetch or
+// build the inverse of their sub-matrix, and emit one decode row per
+// requested missing shard (data rows from the inverse, parity rows as the
+// parity row times the inverse, :620-631).
+int classic_decode_plan(rsgpu_encoder *enc, const uint8_t *present, int data_only,
+                        const uint8_t *required, int n_required, std::vector<uint8_t> &rows,
+                        std::vector<int> &out_idx, std::vector<int> &in_idx) {
+    const int k = enc->k, total = enc->total;
+    rows.clear();
+    out_idx.clear();
+    in_idx.clear();
+    if (required && n_required < k) return RS_ERR_TOO_FEW_SHARDS;
+    auto is_required = [&](int i) {
+        // A required[] of length k covers data shards only; the reference
+        // would index past it for a missing parity shard.
+        return !required || (i < n_required && required[i]);
+    };
+    int number_present = 0, data_present = 0, missing_required = 0;
+    for (int i = 0; i < total; i++) {
+        if (present[i]) {
+            number_present++;
+            if (i < k) data_present++;
+        } else if (required && is_required(i)) {
+            missing_required++;
+        }
+    }
+    if (number_present == 0) return RS_ERR_SHARD_NO_DATA;
+    if (number_present == total || (data_only && data_present == k) ||
+        (required && missing_required == 0))
+        return RS_OK;
+    if (number_present < k) return RS_ERR_TOO_FEW_SHARDS;
+
+    std::vector<int> invalid;
+    for (int r = 0; r < total && (int)in_idx.size() < k; r++) {
+        if (present[r]) in_idx.push_back(r);
+        else invalid.push_back(r);
+    }
+    std::shared_ptr<const Matrix> dec;
+    if (enc->tree) dec = enc->tree->get(invalid);
+    if (!dec) {
+        Matrix sub(k, k);
+        for (int r = 0; r < k; r++)
+            for (int c = 0; c < k; c++) sub.at(r, c) = enc->m.at(in_idx[r], c);
+        auto inv = std::make_shared<Matrix>();
+        int rc = mat_invert(sub, *inv);
+        if (rc) return rc;
+        dec = inv;
+        if (enc->tree) enc->tree->insert(invalid, inv);
+    }
+    const Gf256 &g = Gf256::get();
+    for (int i = 0; i < k; i++)
+        if (!present[i] && is_required(i)) {
+            rows.insert(rows.end(), dec->row(i), dec->row(i) + k);
+            out_idx.push_back(i);
+        }
+    if (!data_only)
+        for (int i = k; i < total; i++)
+            if (!present[i] && is_required(i)) {
+                const uint8_t *pr = enc->m.row(i);
+                for (int j = 0; j < k; j++) {
+                    uint8_t v = 0;
+                    for (int t = 0; t < k; t++) v ^= g.mul[pr[t]][dec->at(t, j)];
+                    rows.push_back(v);
+                }
+                out_idx.push_back(i);
+            }
+    return RS_OK;
+}
+
+static int classic_reconstruct(rsgpu_encoder *enc, uint8_t **shards, const uint8_t *present,
+                               size_t size, int data_only, const uint8_t *required, int n_required,
+                               uint8_t *written) {
+    if (written) memset(written, 0, (size_t)enc->total);
+    if (size == 0) return RS_ERR_SHARD_NO_DATA;
+    std::vector<uint8_t> rows;
+    std::vector<int> out_idx, in_idx;
+    int rc = classic_decode_plan(enc, present, data_only, required, n_required, rows, out_idx, in_idx);
+    if (rc || out_idx.empty()) return rc;
+    rsgpu_ctx *ctx = enc->ctx;
+    std::vector<const uint8_t *> ins(in_idx.size());
+    for (size_t i = 0; i < in_idx.size(); i++) {
+        ins[i] = shards[in_idx[i]];
+        if (!ins[i]) return RS_ERR_SHARD_SIZE;
+    }
+    std::vector<uint8_t *> outs(out_idx.size());
+    for (size_t o = 0; o < out_idx.size(); o++) {
+        uint8_t *&dst = shards[out_idx[o]];
+        if (!dst) {  // no capacity: allocate like AllocAligned (reedsolomon.go:1750)
+            void *pnew = nullptr;
+            RS_CUDA(cudaMalloc(&pnew, size));
+            dst = (uint8_t *)pnew;
+        }
+        outs[o] = dst;
+        if (written) written[out_idx[o]] = 1;
+    }
+    rc = run_matmul(ctx, rows.data(), enc->k, (int)outs.size(), ins.data(), outs.data(), size, kModeWrite);
+    if (rc) return rc;
+    return sync(ctx);
+}
+
+static int check_ptrs(uint8_t *const *shards, int n) {
+    if (!shards) return RS_ERR_TOO_FEW_SHARDS;
+    for (int i = 0; i < n; i++)
+        if (!shards[i]) return RS_ERR_SHARD_SIZE;  // a nil shard has the wrong size (checkShards)
+    return RS_OK;
+}
+
+}  // namespace rsgpu
+
+using namespace rsgpu;
+
+extern "C" {
+
+const char *rsgpu_status_string(int s) {
+    switch (s) {
+    case RS_OK: return "ok";
+    case RS_ERR_TOO_FEW_SHARDS: return "too few shards given";
+    case RS_ERR_SHARD_NO_DATA: return "no shard data";
+    case RS_ERR_SHARD_SIZE: return "shard sizes do not match";
+    case RS_ERR_INVALID_SHARD_SIZE: return "invalid shard size";
+    case RS_ERR_INV_SHARD_NUM: return "cannot create Encoder with less than one data shard or less than zero parity shards";
+    case RS_ERR_MAX_SHARD_NUM: return "cannot create Encoder with more than 256 data+parity shards";
+    case RS_ERR_NOT_SUPPORTED: return "operation not supported";
+    case RS_ERR_INVALID_INPUT: return "invalid input";
+    case RS_ERR_RECONSTRUCT_REQUIRED: return "reconstruction required as one or more required data shards are nil";
+    case RS_ERR_SINGULAR: return "matrix is singular";
+    case RS_ERR_NOT_SQUARE: return "only square matrices can be inverted";
+    case RS_ERR_CUDA: return "CUDA error";
+    case RS_ERR_NOMEM: return "out of device memory";
+    case RS_ERR_TIMEOUT: return "device wait timed out";
+    case RS_ERR_NO_DEVICE: return "encoder has no device context";
+    }
+    return "unknown status";
+}
+
+const char *rsgpu_last_error(void) { return g_last_error.c_str(); }
+
+int rsgpu_ctx_create(int device, rsgpu_ctx **out) {
+    if (!out) return RS_ERR_INVALID_INPUT;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        set_error("no CUDA device");
+        return RS_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= n) return RS_ERR_INVALID_INPUT;
+    RS_CUDA(cudaSetDevice(device));
+    auto *c = new rsgpu_ctx();
+    c->device = device;
+    c->info.device = device;
+    cudaDeviceGetAttribute(&c->info.sm_count, cudaDevAttrMultiProcessorCount, device);
+    cudaError_t e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy_in, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy_out, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_flag, sizeof(int));
+    if (e == cudaSuccess) e = cudaHostAlloc(&c->h_flag, sizeof(int), cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+        int rc = cuda_status(e, "rsgpu_ctx_create");
+        rsgpu_ctx_destroy(c);
+        return rc;
+    }
+    c->stream = c->own_stream;
+    *out = c;
+    return RS_OK;
+}
+
+int rsgpu_ctx_destroy(rsgpu_ctx *c) {
+    if (!c) return RS_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (cudaEvent_t ev : c->events) cudaEventDestroy(ev);
+    c->scratch.release();
+    c->staging.release();
+    if (c->d_flag) cudaFree(c->d_flag);
+    if (c->h_flag) cudaFreeHost(c->h_flag);
+    if (c->copy_in) cudaStreamDestroy(c->copy_in);
+    if (c->copy_out) cudaStreamDestroy(c->copy_out);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+    return RS_OK;
+}
+
+int rsgpu_ctx_set_stream(rsgpu_ctx *c, void *s) {
+    if (!c) return RS_ERR_INVALID_INPUT;
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    c->stream = (cudaStream_t)s;
+    return RS_OK;
+}
+
+int rsgpu_ctx_reset_stream(rsgpu_ctx *c) {
+    if (!c) return RS_ERR_INVALID_INPUT;
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    c->stream = c->own_stream;
+    return RS_OK;
+}
+
+void *rsgpu_ctx_stream(rsgpu_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+int rsgpu_ctx_synchronize(rsgpu_ctx *c) {
+    if (!c) return RS_ERR_INVALID_INPUT;
+    RS_CUDA(cudaStreamSynchronize(c->stream));
+    return RS_OK;
+}
+
+int rsgpu_alloc_shards(rsgpu_ctx *c, int n, size_t each, uint8_t **out) {
+    if (!c || n <= 0 || !out) return RS_ERR_INVALID_INPUT;
+    const size_t pitch = (each + 63) & ~(size_t)63;
+    void *p = nullptr;
+    RS_CUDA(cudaMalloc(&p, pitch * (size_t)n + 64));
+    for (int i = 0; i < n; i++) out[i] = (uint8_t *)p + pitch * (size_t)i;
+    return RS_OK;
+}
+
+int rsgpu_free(rsgpu_ctx *c, void *p) {
+    (void)c;
+    if (p) RS_CUDA(cudaFree(p));
+    return RS_OK;
+}
+
+int rsgpu_host_alloc(size_t bytes, void **out) {
+    if (!out) return RS_ERR_INVALID_INPUT;
+    RS_CUDA(cudaHostAlloc(out, bytes ? bytes : 1, cudaHostAllocPortable));
+    return RS_OK;
+}
+
+int rsgpu_host_free(void *p) {
+    if (p) RS_CUDA(cudaFreeHost(p));
+    return RS_OK;
+}
+
+void rsgpu_options_init(rsgpu_options *o) {
+    if (!o) return;
+    memset(o, 0, sizeof *o);
+    o->matrix_kind = RS_MATRIX_DEFAULT;
+    o->inversion_cache = 1;  // options.go:46-62 defaults
+}
+
+int rsgpu_encoder_new(rsgpu_ctx *ctx, int k, int p, const rsgpu_options *opts, rsgpu_encoder **out) {
+    if (!out) return RS_ERR_INVALID_INPUT;
+    *out = nullptr;
+    rsgpu_options o;
+    if (opts) o = *opts;
+    else rsgpu_options_init(&o);
+    auto enc = std::unique_ptr<rsgpu_encoder>(new rsgpu_encoder());
+    enc->ctx = ctx;
+    enc->k = k;
+    enc->p = p;
+    enc->total = k + p;
+    enc->opts = o;
+    // Codec routing of New (reedsolomon.go:436-443).
+    if ((o.leopard == RS_LEOPARD_GF16 && p > 0) || k + p > 256) {
+        enc->codec = RS_CODEC_LEOPARD16;
+    } else if (o.leopard == RS_LEOPARD_ALWAYS && p > 0) {
+        enc->codec = RS_CODEC_LEOPARD8;
+    }
+    if (enc->codec != RS_CODEC_CLASSIC) {
+        int rc = leo_create(enc.get());
+        if (rc) return rc;
+        *out = enc.release();
+        return RS_OK;
+    }
+    if (k <= 0 || p < 0) return RS_ERR_INV_SHARD_NUM;
+    if (p > 0) {
+        if (o.custom_matrix) {  // reedsolomon.go:469-484
+            if (o.custom_rows < p || o.custom_cols < k) return RS_ERR_INVALID_INPUT;
+            enc->m = Matrix(k + p, k);
+            for (int i = 0; i < k; i++) enc->m.at(i, i) = 1;
+            for (int r = 0; r < p; r++)
+                for (int c = 0; c < k; c++) enc->m.at(k + r, c) = o.custom_matrix[(size_t)r * o.custom_cols + c];
+        } else if (o.fast_one_parity && p == 1) {
+            enc->m = xor_matrix(k);
+        } else {
+            int rc = build_encoding_matrix(o.matrix_kind, k, k + p, enc->m);
+            if (rc) return rc;
+        }
+        enc->parity_rows.assign(enc->m.v.begin() + (size_t)k * k, enc->m.v.end());
+        if (o.inversion_cache) enc->tree.reset(new InversionTree(k, p));
+    }
+    *out = enc.release();
+    return RS_OK;
+}
+
+int rsgpu_encoder_free(rsgpu_encoder *enc) {
+    delete enc;
+    return RS_OK;
+}
+
+int rsgpu_encoder_info(const rsgpu_encoder *enc, int *k, int *p, int *mult, int *codec) {
+    if (!enc) return RS_ERR_INVALID_INPUT;
+    if (k) *k = enc->k;
+    if (p) *p = enc->p;
+    if (mult) *mult = enc->codec == RS_CODEC_CLASSIC ? 1 : 64;  // ShardSizeMultiple
+    if (codec) *codec = enc->codec;
+    return RS_OK;
+}
+
+int rsgpu_encoder_matrix(const rsgpu_encoder *enc, uint8_t *out) {
+    if (!enc || !out) return RS_ERR_INVALID_INPUT;
+    if (enc->codec != RS_CODEC_CLASSIC) return RS_ERR_NOT_SUPPORTED;
+    if (enc->m.v.empty()) return RS_OK;
+    memcpy(out, enc->m.v.data(), enc->m.v.size());
+    return RS_OK;
+}
+
+#define NEED_CTX(enc)                                  \
+    do {                                               \
+        if (!(enc)) return RS_ERR_INVALID_INPUT;       \
+        if (!(enc)->ctx) return RS_ERR_NO_DEVICE;      \
+    } while (0)
+
+int rsgpu_encode(rsgpu_encoder *enc, uint8_t *const *shards, size_t size) {
+    NEED_CTX(enc);
+    std::lock_guard<std::recursive_mutex> lk(enc->ctx->mu);
+    int rc = check_ptrs(shards, enc->total);
+    if (rc) return rc;
+    if (size == 0) return RS_ERR_SHARD_NO_DATA;
+    if (enc->codec != RS_CODEC_CLASSIC) return leo_encode(enc, shards, size);
+    if (enc->p == 0) return RS_OK;
+    rc = run_matmul(enc->ctx, enc->parity_rows.data(), enc->k, enc->p,
+                    (const uint8_t *const *)shards, shards + enc->k, size, kModeWrite);
+    if (rc) return rc;
+    return sync(enc->ctx);
+}
+
+int rsgpu_encode_async(rsgpu_encoder *enc, uint8_t *const *shards, size_t size) {
+    NEED_CTX(enc);
+    std::lock_guard<std::recursive_mutex> lk(enc->ctx->mu);
+    int rc = check_ptrs(shards, enc->total);
+    if (rc) return rc;
+    if (size == 0) return RS_ERR_SHARD_NO_DATA;
+    if (enc->codec != RS_CODEC_CLASSIC) {
+        if (size % 64) return RS_ERR_INVALID_SHARD_SIZE;
+        return leo_encode_enqueue(enc, shards, size);
+    }
+    if (enc->p == 0) return RS_OK;
+    return run_matmul(enc->ctx, enc->parity_rows.data(), enc->k, enc->p,
+                      (const uint8_t *const *)shards, shards + enc->k, size, kModeWrite);
+}
+
+int rsgpu_reconstruct_async(rsgpu_encoder *enc, uint8_t *const *shards, const uint8_t *present,
+                            size_t size, int data_only) {
+    NEED_CTX(enc);
+    if (!shards || !present) return RS_ERR_TOO_FEW_SHARDS;
+    std::lock_guard<std::recursive_mutex> lk(enc->ctx->mu);
+    if (size == 0) return RS_ERR_SHARD_NO_DATA;
+    if (enc->codec != RS_CODEC_CLASSIC) {
+        if (size % 64) return RS_ERR_INVALID_SHARD_SIZE;
+        return leo_reconstruct_enqueue(enc, shards, present, size, !data_only);
+    }
+    std::vector<uint8_t> rows;
+    std::vector<int> out_idx, in_idx;
+    int rc = classic_decode_plan(enc, present, data_only, nullptr, 0, rows, out_idx, in_idx);
+    if (rc || out_idx.empty()) return rc;
+    std::vector<const uint8_t *> ins(in_idx.size());
+    std::vector<uint8_t *> outs(out_idx.size());
+    for (size_t i = 0; i < in_idx.size(); i++) ins[i] = shards[in_idx[i]];
+    for (size_t o = 0; o < out_idx.size(); o++) outs[o] = shards[out_idx[o]];
+    for (auto *q : ins) if (!q) return RS_ERR_SHARD_SIZE;
+    for (auto *q : outs) if (!q) return RS_ERR_INVALID_INPUT;
+    return run_matmul(enc->ctx, rows.data(), enc->k, (int)outs.size(), ins.data(), outs.data(), size,
+                      kModeWrite);
+}
+
+int rsgpu_encode_idx(rsgpu_encoder *enc, const uint8_t *data, int idx, uint8_t *const *parity,
+                     size_t size) {
+    NEED_CTX(enc);
+    if (enc->codec != RS_CODEC_CLASSIC) return RS_ERR_NOT_SUPPORTED;  // leopard.go:272
+    std::lock_guard<std::recursive_mutex> lk(enc->ctx->mu);
+    if (enc->p == 0) return RS_OK;
+    if (idx < 0 || idx >= enc->k) return RS_ERR_INV_SHARD_NUM;
+    int rc = check_ptrs(parity, enc->p);
+    if (rc) return rc;
+    if (!data) return RS_ERR_SHARD_SIZE;
+    if (size == 0) return RS_ERR_SHARD_NO_DATA;
+    std::vector<uint8_t> col(enc->p);
+    for (int o = 0; o < enc->p; o++) col[o] = enc->parity_rows[(size_t)o * enc->k + idx];
+    rc = run_matmul(enc->ctx, col.data(), 1, enc->p, &data, parity, size, kModeXor);
+    if (rc) return rc;
+    return sync(enc->ctx);
+}
+
+int rsgpu_verify(rsgpu_encoder *enc, uint8_t *const *shards, size_t size, int *ok) {
+    NEED_CTX(enc);
+    if (!ok) return RS_ERR_INVALID_INPUT;
+    std::lock_guard<std::recursive_mutex> lk(enc->ctx->mu);
+    *ok = 0;
+    int rc = check_ptrs(shards, enc->total);
+    if (rc) return rc;
+    if (size == 0) return RS_ERR_SHARD_NO_DATA;
+    if (enc->codec != RS_CODEC_CLASSIC) return leo_verify(enc, shards, size, ok);
+    if (enc->p == 0) {
+        *ok = 1;
+        return RS_OK;
+    }
+    return check_shards(enc->ctx, enc->parity_rows.data(), enc->k, enc->p,
+                        (const uint8_t *const *)shards, (const uint8_t *const *)shards + enc->k, size, ok);
+}
+
+static int reconstruct_common(rsgpu_encoder *enc, uint8_t **shards, const uint8_t *present,
+                              size_t size, int data_only, const uint8_t *required, int n_required,
+                              uint8_t *written) {
+    NEED_CTX(enc);
+    if (!shards || !present) return RS_ERR_TOO_FEW_SHARDS;
+    std::lock_guard<std::recursive_mutex> lk(enc->ctx->mu);
+    if (enc->codec != RS_CODEC_CLASSIC) {
+        // leopard.go:378-391: ReconstructSome recovers parity only when
+        // required covers every shard; it is otherwise data-only.
+        int recover_all = !data_only;
+        if (required) recover_all = (n_required == enc->total);
+        return leo_reconstruct(enc, shards, present, size, recover_all, written);
+    }
+    return classic_reconstruct(enc, shards, present, size, data_only, required, n_required, written);
+}
+
+int rsgpu_reconstruct(rsgpu_encoder *enc, uint8_t **shards, const uint8_t *present, size_t size,
+                      uint8_t *written) {
+    return reconstruct_common(enc, shards, present, size, 0, nullptr, 0, written);
+}
+
+int rsgpu_reconstruct_data(rsgpu_encoder *enc, uint8_t **shards, const uint8_t *present,
+                           size_t size, uint8_t *written) {
+    return reconstruct_common(enc, shards, present, size, 1, nullptr, 0, written);
+}
+
+int rsgpu_reconstruct_some(rsgpu_encoder *enc, uint8_t **shards, const uint8_t *present,
+                           const uint8_t *required, int n_required, size_t size, uint8_t *written) {
+    if (!enc) return RS_ERR_INVALID_INPUT;
+    // reedsolomon.go:1655-1660
+    if (!required || (n_required != enc->k && n_required != enc->total)) return RS_ERR_INVALID_INPUT;
+    return reconstruct_common(enc, shards, present, size, n_required == enc->k, required,
+                              n_required, written);
+}
+
+int rsgpu_decode_plan(rsgpu_encoder *enc, const uint8_t *present, int data_only,
+                      const uint8_t *required, int n_required, uint8_t *rows_out, int *out_idx,
+                      int *n_out, int *in_idx) {
+    if (!enc || !present || !n_out) return RS_ERR_INVALID_INPUT;
+    if (enc->codec != RS_CODEC_CLASSIC) return RS_ERR_NOT_SUPPORTED;
+    std::vector<uint8_t> rows;
+    std::vector<int> oi, ii;
+    int rc = classic_decode_plan(enc, present, data_only, required, n_required, rows, oi, ii);
+    *n_out = (int)oi.size();
+    if (rc) return rc;
+    if (rows_out) memcpy(rows_out, rows.data(), rows.size());
+    if (out_idx) memcpy(out_idx, oi.data(), oi.size() * sizeof(int));
+    if (in_idx) memcpy(in_idx, ii.data(), ii.size() * sizeof(int));
+    return RS_OK;
+}
+
+int rsgpu_code_some_shards(rsgpu_ctx *ctx, const uint8_t *rows, int n_in, int n_out,
+                           const uint8_t *const *in, uint8_t *const *out, size_t start, size_t stop,
+                           int clear) {
+    if (!ctx) return RS_ERR_NO_DEVICE;
+    if (!rows || !in || !out || n_in <= 0 || n_out < 0 || stop < start) return RS_ERR_INVALID_INPUT;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    if (n_out == 0 || stop == start) return RS_OK;
+    std::vector<const uint8_t *> ins(n_in);
+    std::vector<uint8_t *> outs(n_out);
+    for (int i = 0; i < n_in; i++) ins[i] = in[i] + start;
+    for (int o = 0; o < n_out; o++) outs[o] = out[o] + start;
+    int rc = run_matmul(ctx, rows, n_in, n_out, ins.data(), outs.data(), stop - start,
+                        clear ? kModeWrite : kModeXor);
+    if (rc) return rc;
+    return sync(ctx);
+}
+
+int rsgpu_check_some_shards(rsgpu_ctx *ctx, const uint8_t *rows, int n_in, int n_out,
+                            const uint8_t *const *in, const uint8_t *const *to_check, size_t nbytes,
+                            int *ok) {
+    if (!ctx) return RS_ERR_NO_DEVICE;
+    if (!ok || !rows || !in || !to_check || n_in <= 0 || n_out < 0) return RS_ERR_INVALID_INPUT;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    if (n_out == 0 || nbytes == 0) {
+        *ok = 1;
+        return RS_OK;
+    }
+    return check_shards(ctx, rows, n_in, n_out, in, to_check, nbytes, ok);
+}
+
+int rsgpu_gal_mul_slice(rsgpu_ctx *ctx, uint8_t c, const uint8_t *in, uint8_t *out, size_t n,
+                        int xor_into) {
+    if (!ctx) return RS_ERR_NO_DEVICE;
+    if (!in || !out) return RS_ERR_INVALID_INPUT;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    int rc = run_matmul(ctx, &c, 1, 1, &in, &out, n, xor_into ? kModeXor : kModeWrite);
+    if (rc) return rc;
+    return sync(ctx);
+}
+
+int rsgpu_slice_xor(rsgpu_ctx *ctx, const uint8_t *in, uint8_t *out, size_t n) {
+    if (!ctx) return RS_ERR_NO_DEVICE;
+    if (!in || !out) return RS_ERR_INVALID_INPUT;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    RS_CUDA(launch_xor(ctx->stream, ctx->info, in, out, n));
+    return sync(ctx);
+}
+
+int rsgpu_autotune_gf8(rsgpu_ctx *ctx, int n_in, int n_out, size_t nbytes, int mode, int reps,
+                       float *ms_out, int *best_out) {
+    if (!ctx) return RS_ERR_NO_DEVICE;
+    if (n_in <= 0 || n_in > kMaxIn || n_out <= 0 || n_out > kMaxOut || nbytes == 0 || mode < 0 ||
+        mode > kModeVerify)
+        return RS_ERR_INVALID_INPUT;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    if (reps < 1) reps = 3;
+    const size_t pitch = (nbytes + 255) & ~(size_t)255;
+    int rc = ctx->scratch.ensure(pitch * (size_t)(n_in + n_out));
+    if (rc) return rc;
+    RS_CUDA(cudaMemsetAsync(ctx->scratch.ptr, 0x5A, pitch * (size_t)(n_in + n_out), ctx->stream));
+    std::vector<const uint8_t *> ins(n_in);
+    std::vector<uint8_t *> outs(n_out);
+    for (int i = 0; i < n_in; i++) ins[i] = ctx->scratch.ptr + pitch * i;
+    for (int o = 0; o < n_out; o++) outs[o] = ctx->scratch.ptr + pitch * (n_in + o);
+    std::vector<uint8_t> rows((size_t)n_in * n_out);
+    for (size_t i = 0; i < rows.size(); i++) rows[i] = (uint8_t)(37 * i + 11) | 1;
+    GfMatArgs a;
+    fill_args(a, rows.data(), n_in, n_in, n_out, ins.data(), outs.data(), nbytes, ctx->d_flag);
+    cudaEvent_t e0, e1;
+    RS_CUDA(cudaEventCreate(&e0));
+    RS_CUDA(cudaEventCreate(&e1));
+    float best_ms = 1e30f;
+    int best = kVariantFixed;
+    for (int v = 0; v < kNumVariants; v++) {
+        RS_CUDA(launch_gf8_tile(ctx->stream, ctx->info, a, mode, v));  // warm
+        RS_CUDA(cudaEventRecord(e0, ctx->stream));
+        for (int r = 0; r < reps; r++) RS_CUDA(launch_gf8_tile(ctx->stream, ctx->info, a, mode, v));
+        RS_CUDA(cudaEventRecord(e1, ctx->stream));
+        RS_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        RS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        ms /= reps;
+        if (ms_out) ms_out[v] = ms;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = v;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    record_variant(n_in, n_out, mode, nbytes, best);
+    if (best_out) *best_out = best;
+    return RS_OK;
+}
+
+int rsgpu_force_variant(int v) {
+    if (v >= kNumVariants) return RS_ERR_INVALID_INPUT;
+    set_forced_variant(v);
+    return RS_OK;
+}
+
+int rsgpu_num_variants(void) { return kNumVariants; }
+
+int rsgpu_build_matrix(int kind, int k, int total, uint8_t *out) {
+    if (!out) return RS_ERR_INVALID_INPUT;
+    Matrix m;
+    int rc = build_encoding_matrix(kind, k, total, m);
+    if (rc) return rc;
+    memcpy(out, m.v.data(), m.v.size());
+    return RS_OK;
+}
+
+int rsgpu_invert_matrix(const uint8_t *m, int n, uint8_t *out) {
+    if (!m || !out || n <= 0) return RS_ERR_INVALID_INPUT;
+    Matrix a(n, n), inv;
+    memcpy(a.v.data(), m, (size_t)n * n);
+    int rc = mat_invert(a, inv);
+    if (rc) return rc;
+    memcpy(out, inv.v.data(), (size_t)n * n);
+    return RS_OK;
+}
+
+uint8_t rsgpu_gal_mul(uint8_t a, uint8_t b) { return gf_mul(a, b); }
+
+}  // extern "C"

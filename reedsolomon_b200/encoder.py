@@ -1,0 +1,416 @@
+"""Python mirror of the reference's Encoder interface on top of librsgpu.so.
+
+    enc = New(10, 4)                     # reedsolomon.New(10, 4)
+    enc.Encode(shards)                   # shards: 14 CUDA uint8 tensors
+    ok = enc.Verify(shards)
+    shards[3] = None                     # a missing shard, like a nil slice
+    enc.Reconstruct(shards)              # fills shards[3] in place
+
+Shards are 1-D contiguous torch.uint8 tensors.  CUDA tensors run the device
+path; CPU tensors / numpy arrays run the host path (PCIe copies inside the
+library).  Errors raise the exception named after the reference's sentinel
+error (ErrTooFewShards, ErrShardSize, ...).
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+RS_CODEC_CLASSIC, RS_CODEC_LEOPARD16, RS_CODEC_LEOPARD8 = 0, 1, 2
+_MATRIX = {"default": 0, "cauchy": 1, "par1": 2, "jerasure": 3}
+
+
+class RSError(Exception):
+    code = None
+
+
+def _err(name, code):
+    return type(name, (RSError,), {"code": code})
+
+
+ErrTooFewShards = _err("ErrTooFewShards", -1)
+ErrShardNoData = _err("ErrShardNoData", -2)
+ErrShardSize = _err("ErrShardSize", -3)
+ErrInvalidShardSize = _err("ErrInvalidShardSize", -4)
+ErrInvShardNum = _err("ErrInvShardNum", -5)
+ErrMaxShardNum = _err("ErrMaxShardNum", -6)
+ErrNotSupported = _err("ErrNotSupported", -7)
+ErrInvalidInput = _err("ErrInvalidInput", -8)
+ErrReconstructRequired = _err("ErrReconstructRequired", -9)
+ErrSingular = _err("ErrSingular", -10)
+ErrNotSquare = _err("ErrNotSquare", -11)
+CudaError = _err("CudaError", -100)
+ErrNoMem = _err("ErrNoMem", -101)
+ErrTimeout = _err("ErrTimeout", -102)
+ErrNoDevice = _err("ErrNoDevice", -103)
+_BY_CODE = {c.code: c for c in (ErrTooFewShards, ErrShardNoData, ErrShardSize, ErrInvalidShardSize,
+                                ErrInvShardNum, ErrMaxShardNum, ErrNotSupported, ErrInvalidInput,
+                                ErrReconstructRequired, ErrSingular, ErrNotSquare, CudaError, ErrNoMem,
+                                ErrTimeout, ErrNoDevice)}
+
+
+def check(rc):
+    if rc != 0:
+        lib = L.lib()
+        msg = lib.rsgpu_status_string(rc).decode()
+        detail = lib.rsgpu_last_error().decode()
+        exc = _BY_CODE.get(rc, RSError)
+        raise exc("%s%s" % (msg, (": " + detail) if detail and rc <= -100 else ""))
+    return rc
+
+
+# ---- options (options.go) ---------------------------------------------------
+def _opt(**kv):
+    def apply(o):
+        o.update(kv)
+    return apply
+
+
+def WithCauchyMatrix():
+    return _opt(matrix="cauchy")
+
+
+def WithPAR1Matrix():
+    return _opt(matrix="par1")
+
+
+def WithJerasureMatrix():
+    return _opt(matrix="jerasure")
+
+
+def WithFastOneParityMatrix():
+    return _opt(fast_one_parity=1)
+
+
+def WithCustomMatrix(rows):
+    return _opt(custom=np.asarray(rows, dtype=np.uint8))
+
+
+def WithLeopardGF16(enabled=True):
+    return _opt(leopard=1 if enabled else 0)
+
+
+def WithLeopardGF(enabled=True):
+    return _opt(leopard=2 if enabled else 0)
+
+
+def WithInversionCache(enabled=True):
+    return _opt(inversion_cache=1 if enabled else 0)
+
+
+def WithGPU(device=0):
+    """Select the CUDA device (the GPU counterpart of the CPU tuning options)."""
+    return _opt(device=int(device))
+
+
+def _noop(*_a, **_k):
+    return lambda o: None
+
+
+# CPU scheduling / ISA options of the reference: accepted, no effect on a GPU.
+WithMaxGoroutines = WithAutoGoroutines = WithMinSplitSize = _noop
+WithSSSE3 = WithAVX2 = WithSSE2 = WithAVX512 = WithGFNI = WithAVXGFNI = _noop
+WithConcurrentStreams = WithConcurrentStreamReads = WithConcurrentStreamWrites = _noop
+WithStreamBlockSize = WithWorkAllocator = _noop
+
+
+# ---- device contexts ----------------------------------------------------------
+class Context:
+    """One librsgpu context (stream + scratch) per CUDA device, kept for the
+    life of the process (like the reference's package-level tables)."""
+    _by_device = {}
+
+    def __init__(self, device):
+        self.device = device
+        h = ctypes.c_void_p()
+        check(L.lib().rsgpu_ctx_create(device, ctypes.byref(h)))
+        self.handle = h
+
+    @classmethod
+    def get(cls, device=0):
+        if device not in cls._by_device:
+            cls._by_device[device] = cls(device)
+        return cls._by_device[device]
+
+    def bind_current_stream(self):
+        """Run library work on torch's current stream, ordered with torch ops."""
+        s = torch.cuda.current_stream(self.device).cuda_stream
+        check(L.lib().rsgpu_ctx_set_stream(self.handle, ctypes.c_void_p(s)))
+
+
+def _is_device(t):
+    return isinstance(t, torch.Tensor) and t.is_cuda
+
+
+def _size(shards):
+    for s in shards:
+        if s is not None and len(s):
+            return len(s)
+    return 0
+
+
+def _ptr(t):
+    if t is None or len(t) == 0:
+        return None
+    if isinstance(t, np.ndarray):
+        if not t.flags["C_CONTIGUOUS"] or t.dtype != np.uint8:
+            raise ErrInvalidInput("shards must be contiguous uint8")
+        return t.ctypes.data
+    if t.dtype != torch.uint8 or not t.is_contiguous():
+        raise ErrInvalidInput("shards must be contiguous uint8")
+    return t.data_ptr()
+
+
+class Encoder:
+    """Encoder + Extensions (reedsolomon.go:25-165) over librsgpu."""
+
+    def __init__(self, data_shards, parity_shards, opts):
+        o = {"device": 0, "matrix": "default", "fast_one_parity": 0, "leopard": 0,
+             "inversion_cache": 1, "custom": None, "host_only": False}
+        for f in opts:
+            f(o)
+        self._o = o
+        lib = L.lib()
+        ro = L.RsOptions()
+        lib.rsgpu_options_init(ctypes.byref(ro))
+        ro.matrix_kind = _MATRIX[o["matrix"]]
+        ro.fast_one_parity = o["fast_one_parity"]
+        ro.leopard = o["leopard"]
+        ro.inversion_cache = o["inversion_cache"]
+        self._custom = None
+        if o["custom"] is not None:
+            self._custom = np.ascontiguousarray(o["custom"])
+            ro.custom_matrix = self._custom.ctypes.data
+            ro.custom_rows, ro.custom_cols = self._custom.shape
+        self.ctx = None if o["host_only"] else Context.get(o["device"])
+        h = ctypes.c_void_p()
+        check(lib.rsgpu_encoder_new(self.ctx.handle if self.ctx else None, data_shards, parity_shards,
+                                    ctypes.byref(ro), ctypes.byref(h)))
+        self._h = h
+        k, p, mult, codec = (ctypes.c_int() for _ in range(4))
+        check(lib.rsgpu_encoder_info(h, ctypes.byref(k), ctypes.byref(p), ctypes.byref(mult), ctypes.byref(codec)))
+        self._k, self._p, self._mult, self.codec = k.value, p.value, mult.value, codec.value
+
+    def __del__(self):
+        try:
+            L.lib().rsgpu_encoder_free(self._h)
+        except Exception:
+            pass
+
+    # Extensions
+    def DataShards(self):
+        return self._k
+
+    def ParityShards(self):
+        return self._p
+
+    def TotalShards(self):
+        return self._k + self._p
+
+    def ShardSizeMultiple(self):
+        return self._mult
+
+    def Matrix(self):
+        m = np.zeros((self.TotalShards(), self._k), dtype=np.uint8)
+        check(L.lib().rsgpu_encoder_matrix(self._h, m.ctypes.data))
+        return m
+
+    def AllocAligned(self, each):
+        """TotalShards device shards of `each` bytes, 64-byte aligned views of one allocation."""
+        pitch = (each + 63) // 64 * 64
+        buf = torch.empty(pitch * self.TotalShards() + 64, dtype=torch.uint8, device="cuda:%d" % self.ctx.device)
+        base = (-buf.data_ptr()) % 64
+        return [buf[base + i * pitch: base + i * pitch + each] for i in range(self.TotalShards())]
+
+    # --- helpers
+    def _prep(self, shards, nilok):
+        if len(shards) != self.TotalShards():
+            raise ErrTooFewShards("too few shards given")
+        size = _size(shards)
+        if size == 0:
+            raise ErrShardNoData("no shard data")
+        for s in shards:
+            n = 0 if s is None else len(s)
+            if n != size and (n != 0 or not nilok):
+                raise ErrShardSize("shard sizes do not match")
+        dev = any(_is_device(s) for s in shards if s is not None and len(s))
+        return size, dev
+
+    def _bind(self):
+        if self.ctx is None:
+            raise ErrNoDevice("encoder has no device context")
+        self.ctx.bind_current_stream()
+
+    # Encoder
+    def Encode(self, shards):
+        size, dev = self._prep(shards, nilok=False)
+        lib = L.lib()
+        arr = L.ptr_array([_ptr(s) for s in shards])
+        if dev:
+            self._bind()
+            check(lib.rsgpu_encode(self._h, arr, size))
+        else:
+            check(lib.rsgpu_encode_host(self._h, arr, size))
+
+    def EncodeIdx(self, data_shard, idx, parity):
+        if len(parity) != self._p:
+            raise ErrTooFewShards("too few shards given")
+        if self._p == 0:
+            return
+        if idx < 0 or idx >= self._k:
+            raise ErrInvShardNum("invalid shard index")
+        size = _size(parity)
+        if size == 0:
+            raise ErrShardNoData("no shard data")
+        if any(p is None or len(p) != size for p in parity) or len(data_shard) != size:
+            raise ErrShardSize("shard sizes do not match")
+        self._bind()
+        check(L.lib().rsgpu_encode_idx(self._h, _ptr(data_shard), idx,
+                                       L.ptr_array([_ptr(p) for p in parity]), size))
+
+    def Verify(self, shards):
+        size, dev = self._prep(shards, nilok=False)
+        if not dev:
+            raise ErrNotSupported("Verify takes device shards")
+        self._bind()
+        ok = ctypes.c_int()
+        check(L.lib().rsgpu_verify(self._h, L.ptr_array([_ptr(s) for s in shards]), size, ctypes.byref(ok)))
+        return bool(ok.value)
+
+    def _reconstruct(self, shards, data_only, required=None):
+        if len(shards) != self.TotalShards():
+            raise ErrTooFewShards("too few shards given")
+        size, dev = self._prep(shards, nilok=True)
+        present = [1 if (s is not None and len(s)) else 0 for s in shards]
+        n = self.TotalShards()
+        if required is not None:
+            req = [bool(r) for r in required]
+            want = [not present[i] and i < len(req) and req[i] for i in range(n)]
+        else:
+            want = [not present[i] and (i < self._k or not data_only) for i in range(n)]
+        if not dev:
+            return self._reconstruct_host(shards, present, want, size, data_only, required)
+        self._bind()
+        device = self.ctx.device
+        outs = list(shards)
+        for i in range(n):
+            if want[i]:
+                outs[i] = torch.empty(size, dtype=torch.uint8, device="cuda:%d" % device)
+        ptrs = L.ptr_array([_ptr(s) for s in outs])
+        pres = L.u8_array(present)
+        written = (ctypes.c_uint8 * n)()
+        lib = L.lib()
+        if required is not None:
+            reqa = L.u8_array([1 if r else 0 for r in required])
+            check(lib.rsgpu_reconstruct_some(self._h, ptrs, pres, reqa, len(required), size, written))
+        elif data_only:
+            check(lib.rsgpu_reconstruct_data(self._h, ptrs, pres, size, written))
+        else:
+            check(lib.rsgpu_reconstruct(self._h, ptrs, pres, size, written))
+        for i in range(n):
+            if written[i]:
+                shards[i] = outs[i]
+
+    def Reconstruct(self, shards):
+        self._reconstruct(shards, data_only=False)
+
+    def ReconstructData(self, shards):
+        self._reconstruct(shards, data_only=True)
+
+    def ReconstructSome(self, shards, required):
+        if len(required) not in (self._k, self.TotalShards()):
+            raise ErrInvalidInput("invalid input")
+        self._reconstruct(shards, data_only=len(required) == self._k, required=required)
+
+    def _reconstruct_host(self, shards, present, want, size, data_only, required):
+        """Host buffers: missing outputs are allocated as pinned CPU tensors, PCIe copies run inside."""
+        if required is not None:
+            raise ErrNotSupported("ReconstructSome takes device shards")
+        n = self.TotalShards()
+        outs = list(shards)
+        for i in range(n):
+            if want[i]:
+                outs[i] = torch.empty(size, dtype=torch.uint8, pin_memory=True)
+        written = (ctypes.c_uint8 * n)()
+        check(L.lib().rsgpu_reconstruct_host(self._h, L.ptr_array([_ptr(s) for s in outs]),
+                                             L.u8_array(present), size, int(data_only), written))
+        for i in range(n):
+            if written[i]:
+                shards[i] = outs[i]
+
+    def DecodePlan(self, present, data_only=False, required=None):
+        """The decode rows, output and input indices reconstruct would use (host only)."""
+        n, k = self.TotalShards(), self._k
+        rows = np.zeros((n, k), dtype=np.uint8)
+        out_idx = (ctypes.c_int * n)()
+        in_idx = (ctypes.c_int * k)()
+        n_out = ctypes.c_int()
+        req = L.u8_array(required) if required is not None else None
+        check(L.lib().rsgpu_decode_plan(self._h, L.u8_array(present), int(data_only), req,
+                                        len(required) if required is not None else 0,
+                                        rows.ctypes.data, out_idx, ctypes.byref(n_out), in_idx))
+        no = n_out.value
+        return rows[:no].copy(), list(out_idx[:no]), (list(in_idx[:k]) if no else [])
+
+
+def New(data_shards, parity_shards, *opts):
+    """reedsolomon.New (reedsolomon.go:425)."""
+    return Encoder(data_shards, parity_shards, opts)
+
+
+def HostOnly():
+    """Option: build the encoder without a device context (planning only)."""
+    return _opt(host_only=True)
+
+
+# ---- kernel seam (LowLevel / codeSomeShards) ---------------------------------
+def code_some_shards(rows, inputs, outputs, clear=True, start=0, stop=None, device=0):
+    rows = np.ascontiguousarray(rows, dtype=np.uint8)
+    n_out, n_in = rows.shape
+    ctx = Context.get(device)
+    ctx.bind_current_stream()
+    stop = len(inputs[0]) if stop is None else stop
+    check(L.lib().rsgpu_code_some_shards(ctx.handle, rows.ctypes.data, n_in, n_out,
+                                         L.ptr_array([t.data_ptr() for t in inputs]),
+                                         L.ptr_array([t.data_ptr() for t in outputs]),
+                                         start, stop, int(bool(clear))))
+
+
+def check_some_shards(rows, inputs, to_check, device=0):
+    rows = np.ascontiguousarray(rows, dtype=np.uint8)
+    n_out, n_in = rows.shape
+    ctx = Context.get(device)
+    ctx.bind_current_stream()
+    ok = ctypes.c_int()
+    check(L.lib().rsgpu_check_some_shards(ctx.handle, rows.ctypes.data, n_in, n_out,
+                                          L.ptr_array([t.data_ptr() for t in inputs]),
+                                          L.ptr_array([t.data_ptr() for t in to_check]),
+                                          len(inputs[0]), ctypes.byref(ok)))
+    return bool(ok.value)
+
+
+def gal_mul_slice(c, inp, out, xor=False, device=0):
+    ctx = Context.get(device)
+    ctx.bind_current_stream()
+    check(L.lib().rsgpu_gal_mul_slice(ctx.handle, int(c), inp.data_ptr(), out.data_ptr(), len(inp), int(xor)))
+
+
+def slice_xor(inp, out, device=0):
+    ctx = Context.get(device)
+    ctx.bind_current_stream()
+    check(L.lib().rsgpu_slice_xor(ctx.handle, inp.data_ptr(), out.data_ptr(), len(inp)))
+
+
+def build_matrix(kind, data_shards, total_shards):
+    out = np.zeros((total_shards, data_shards), dtype=np.uint8)
+    check(L.lib().rsgpu_build_matrix(_MATRIX[kind], data_shards, total_shards, out.ctypes.data))
+    return out
+
+
+def invert_matrix(m):
+    m = np.ascontiguousarray(m, dtype=np.uint8)
+    out = np.zeros_like(m)
+    check(L.lib().rsgpu_invert_matrix(m.ctypes.data, m.shape[0], out.ctypes.data))
+    return out

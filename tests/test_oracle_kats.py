@@ -1,0 +1,156 @@
+"""Pin the CPU oracle against the reference's own golden vectors (CPU only).
+
+Fixtures in tests/golden/reference_kats.json were extracted from the
+reference's sources by tests/golden/make_golden.py.
+"""
+import hashlib
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+
+def test_gf8_tables_match_reference_literals(kats):
+    # galois.go:29 logTable, :71 expTable, :78 invTable, :337/:593 mulTableLow/High, :80 mulTable
+    log, exp, inv, low, high = O.gf8_tables()
+    t = kats["tables"]
+    assert list(log) == t["logTable"]
+    assert list(exp) == t["expTable"]
+    assert list(inv) == t["invTable"]
+    assert list(low) == t["mulTableLow"]
+    assert list(high) == t["mulTableHigh"]
+    assert hashlib.sha256(O.gf8_multable().tobytes()).hexdigest() == t["mulTable_sha256"]
+
+
+def test_gfni_matrices_match_reference(kats):
+    # galois.go:948 gf2p811dMulMatrices pins "multiply by c" bit-for-bit
+    t = kats["tables"]["gf2p811dMulMatrices"]
+    assert [O.gfni_matrix(c) for c in range(256)] == t
+
+
+def test_leopard8_field_matches_reference_gfni(kats):
+    # leopard8.go:1271 gf2p811dMulMatricesLeo8 pins the Cantor-basis log/exp and mulLog8
+    t = kats["tables"]["gf2p811dMulMatricesLeo8"]
+    assert [O.lib().ora_leo8_gfni_matrix(m) for m in range(256)] == t
+
+
+def test_galois_kats(kats):
+    g = kats["galois"]
+    for a, b, r in g["mul"]:
+        assert O.gal_mul(a, b) == r
+    for a, n, r in g["exp"]:
+        assert O.gal_exp(a, n) == r
+    inp = np.array(g["in"], np.uint8)
+    out = np.zeros_like(inp)
+    for s in g["slices"]:  # galois_test.go:127-174 sequence (xor steps reuse out)
+        O.gal_mul_slice(s["c"], inp, out, xor=s["xor"])
+        assert list(out) == s["expect"], s["c"]
+
+
+def test_one_encode(kats):
+    oe = kats["one_encode"]
+    sh = [np.array(s, np.uint8) for s in oe["shards"]]
+    assert O.rs_encode(oe["k"], oe["p"], sh) == 0
+    for i, v in oe["parity"].items():
+        assert list(sh[int(i)]) == v
+    rc, ok = O.rs_verify(oe["k"], oe["p"], sh)
+    assert rc == 0 and ok
+    sh[8][0] ^= 1
+    assert not O.rs_verify(oe["k"], oe["p"], sh)[1]
+
+
+def test_matrix_kats(kats):
+    m = kats["matrix"]
+    prod = O.mat_multiply(m["multiply"]["a"], m["multiply"]["b"])
+    assert str(prod.tolist()).replace(" ", "") == m["multiply"]["expect"].replace(" ", "")
+    for case in m["inverse"]:
+        rc, inv = O.invert(np.array(case["m"], np.uint8))
+        assert rc == 0
+        assert str(inv.tolist()).replace(" ", "") == case["inverse"].replace(" ", "")
+    for s in m["singular"]:
+        assert O.invert(np.array(s, np.uint8))[0] == -10  # errSingular
+
+
+def test_jerasure_matrix(kats):
+    j = kats["jerasure"]
+    rc, m = O.build_matrix("jerasure", j["k"], j["total"])
+    assert rc == 0
+    assert (m[:j["k"]] == np.eye(j["k"], dtype=np.uint8)).all()
+    assert m[j["k"]:].tolist() == j["parity_rows"]
+
+
+def test_addmod_kats(kats):
+    # leopard_test.go:167-190 / leopard8_test.go:10-33 through the oracle's FWHT butterflies:
+    # addMod is exercised via mulLog; here the raw definition is checked in Python and the
+    # oracle's tables must satisfy it on the reference's cases.
+    for x, y, e in kats["addmod16"]:
+        s = x + y
+        assert (s + (s >> 16)) & 0xFFFF == e
+    for x, y, e in kats["addmod8"]:
+        s = x + y
+        assert (s + (s >> 8)) & 0xFF == e
+
+
+@pytest.mark.parametrize("kind", ["default", "cauchy", "par1", "jerasure"])
+def test_matrix_kinds_systematic(kind):
+    for k, total in [(1, 2), (5, 8), (10, 14), (17, 20)]:
+        rc, m = O.build_matrix(kind, k, total)
+        assert rc == 0
+        assert (m[:k] == np.eye(k, dtype=np.uint8)).all()
+
+
+def test_oracle_roundtrip_classic():
+    k, p, size = 10, 4, 1000
+    sh = O.seeded_shards(7, k, size) + [np.zeros(size, np.uint8) for _ in range(p)]
+    assert O.rs_encode(k, p, sh) == 0
+    orig = [s.copy() for s in sh]
+    present = [1] * (k + p)
+    for i in (0, 3, 11, 13):
+        present[i] = 0
+        sh[i][:] = 0
+    rc, written = O.rs_reconstruct(k, p, sh, present)
+    assert rc == 0
+    assert all((a == b).all() for a, b in zip(sh, orig))
+    assert [i for i, w in enumerate(written) if w] == [0, 3, 11, 13]
+
+
+def test_oracle_fast_matches_scalar():
+    rng = np.random.default_rng(3)
+    for n_in, n_out, size in [(10, 4, 4096 + 17), (3, 9, 333), (32, 8, 1 << 14), (1, 1, 65)]:
+        rows = rng.integers(0, 256, (n_out, n_in), dtype=np.uint8)
+        ins = [rng.integers(0, 256, size, dtype=np.uint8) for _ in range(n_in)]
+        a = [np.zeros(size, np.uint8) for _ in range(n_out)]
+        b = [np.zeros(size, np.uint8) for _ in range(n_out)]
+        O.code_some_shards(rows, ins, a)
+        O.code_some_shards_fast(rows, ins, b, threads=3)
+        assert all((x == y).all() for x, y in zip(a, b))
+
+
+LEO_CASES = [(16, 5, 3, 128), (16, 20, 13, 192), (16, 300, 60, 128), (8, 5, 3, 128), (8, 40, 24, 256),
+             (8, 192, 56, 128)]
+
+
+@pytest.mark.parametrize("gf,k,p,size", LEO_CASES)
+def test_oracle_leopard_roundtrip(gf, k, p, size):
+    rng = np.random.default_rng(k * 31 + p)
+    sh = [rng.integers(0, 256, size, dtype=np.uint8) for _ in range(k)] + [np.zeros(size, np.uint8) for _ in range(p)]
+    assert O.leo_encode(gf, k, p, sh) == 0
+    rc, ok = O.leo_verify(gf, k, p, sh)
+    assert rc == 0 and ok
+    orig = [s.copy() for s in sh]
+    lost = rng.choice(k + p, size=p, replace=False)
+    present = [1] * (k + p)
+    for i in lost:
+        present[i] = 0
+        sh[i][:] = 0
+    rc, written = O.leo_reconstruct(gf, k, p, sh, present, recover_all=True)
+    assert rc == 0
+    assert all((a == b).all() for a, b in zip(sh, orig))
+    assert sorted(i for i, w in enumerate(written) if w) == sorted(int(i) for i in lost)
+
+
+def test_oracle_leopard8_rejects_overlong_geometry():
+    # 200+56: ceilPow2(56)+200 > 256 indexes past the reference's tables (leopard8.go:151,441)
+    sh = [np.zeros(64, np.uint8) for _ in range(256)]
+    assert O.leo_encode(8, 200, 56, sh) == -6
