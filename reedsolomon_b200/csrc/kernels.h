@@ -63,6 +63,10 @@ cudaError_t launch_gf8_matmul(cudaStream_t st, const DeviceInfo &dev, const uint
                               int n_out, const uint8_t *const *in, uint8_t *const *out,
                               size_t nbytes, int mode, int *d_flag);
 
+// Fill an 8-byte aligned buffer with uniform pseudo-random bytes (tuning inputs).
+cudaError_t launch_fill_random(cudaStream_t st, const DeviceInfo &dev, uint8_t *p, size_t nbytes,
+                               uint64_t seed);
+
 // out ^= in (sliceXor)
 cudaError_t launch_xor(cudaStream_t st, const DeviceInfo &dev, const uint8_t *in, uint8_t *out,
                        size_t nbytes);

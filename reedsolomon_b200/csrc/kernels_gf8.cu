@@ -362,6 +362,18 @@ __global__ void __launch_bounds__(kThreads) xor_bytes(const uint8_t *__restrict_
         out[p] ^= in[p];
 }
 
+// Uniform pseudo-random bytes (splitmix64 of the word index and a seed), so
+// tuning runs see lookups spread like real shard data.
+__global__ void __launch_bounds__(kThreads) fill_random(uint64_t *p, long long nwords, uint64_t seed) {
+    for (long long i = (long long)blockIdx.x * kThreads + threadIdx.x; i < nwords;
+         i += (long long)gridDim.x * kThreads) {
+        uint64_t z = seed + (uint64_t)i * 0x9E3779B97F4A7C15ull;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        p[i] = z ^ (z >> 31);
+    }
+}
+
 typedef void (*VecKernel)(GfMatArgs);
 typedef void (*ByteKernel)(GfMatArgs, long long);
 
@@ -548,6 +560,15 @@ cudaError_t launch_gf8_matmul(cudaStream_t st, const DeviceInfo &dev, const uint
         }
     }
     return cudaSuccess;
+}
+
+cudaError_t launch_fill_random(cudaStream_t st, const DeviceInfo &dev, uint8_t *p, size_t nbytes,
+                               uint64_t seed) {
+    const long long nwords = (long long)(nbytes / 8);
+    if (nwords == 0) return cudaSuccess;
+    const int grid = (int)std::min<long long>((nwords + kThreads - 1) / kThreads, (long long)dev.sm_count * 8);
+    fill_random<<<grid, kThreads, 0, st>>>(reinterpret_cast<uint64_t *>(p), nwords, seed);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_xor(cudaStream_t st, const DeviceInfo &dev, const uint8_t *in, uint8_t *out,
