@@ -161,6 +161,19 @@ int rsgpu_code_some_shards(rsgpu_ctx *ctx, const uint8_t *rows, int n_in, int n_
 int rsgpu_check_some_shards(rsgpu_ctx *ctx, const uint8_t *rows, int n_in, int n_out,
                             const uint8_t *const *in, const uint8_t *const *to_check,
                             size_t nbytes, int *ok);
+/* No counterpart in the reference.  checkSomeShards for callers that cannot
+ * allocate device memory (a process that reserved its whole HBM budget up
+ * front, or a latency-critical path that must not risk cudaMalloc): no
+ * context, no allocation.  Its scratch is one 8 MiB array per device, static in
+ * the library and held until exit; more than 32 inputs need
+ * n_out * round_up(nbytes, 256) <= 8 MiB - 256, larger calls return
+ * RS_ERR_INVALID_INPUT.  Runs on `cuda_stream` on the current device and
+ * waits for it.  The first call on a device looks up the array's device
+ * address; make it before any stream capture.  Calls that overlap on the GPU
+ * share the array and race: serialise them. */
+int rsgpu_check_some_shards_noalloc(const uint8_t *rows, int n_in, int n_out,
+                                    const uint8_t *const *in, const uint8_t *const *to_check,
+                                    size_t nbytes, void *cuda_stream, int *ok);
 /* galMulSlice / galMulSliceXor (galois_amd64.go:49-159; mulslice.go:29-38) */
 int rsgpu_gal_mul_slice(rsgpu_ctx *ctx, uint8_t c, const uint8_t *in, uint8_t *out, size_t n,
                         int xor_into);

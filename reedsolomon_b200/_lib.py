@@ -60,6 +60,7 @@ SIGNATURES = {
     "rsgpu_decode_plan": (c_int, [c_voidp, c_voidp, c_int, c_voidp, c_int, c_voidp, c_voidp, c_intp, c_voidp]),
     "rsgpu_code_some_shards": (c_int, [c_voidp, c_voidp, c_int, c_int, c_voidp, c_voidp, c_size, c_size, c_int]),
     "rsgpu_check_some_shards": (c_int, [c_voidp, c_voidp, c_int, c_int, c_voidp, c_voidp, c_size, c_intp]),
+    "rsgpu_check_some_shards_noalloc": (c_int, [c_voidp, c_int, c_int, c_voidp, c_voidp, c_size, c_voidp, c_intp]),
     "rsgpu_gal_mul_slice": (c_int, [c_voidp, ctypes.c_uint8, c_voidp, c_voidp, c_size, c_int]),
     "rsgpu_slice_xor": (c_int, [c_voidp, c_voidp, c_voidp, c_size]),
     "rsgpu_autotune_gf8": (c_int, [c_voidp, c_int, c_int, c_size, c_int, c_int, c_voidp, c_intp]),
