@@ -1,21 +1,582 @@
-// leopard.cu -- Leopard GF(2^16) / GF(2^8) codecs (placeholder until the FFT kernels land).
+// leopard.cu -- Leopard GF(2^16) / GF(2^8) FFT codec on sm_100a.
+//
+// Replaces leopardFF16.encode/reconstruct (leopard.go:169-647) and
+// leopardFF8.encode/reconstruct (leopard8.go:139-634) and their SIMD
+// butterflies (fftDIT4/ifftDIT4/fftDIT48/..., galois_amd64.go:206-1164).
+//
+// Every transform is column-local: one CTA owns a 64-byte column tile of
+// every row (for GF(2^16) one chunk: 32 symbols as 32 low bytes | 32 high
+// bytes, leopard.go:907-925; for GF(2^8) 64 byte symbols) and runs all
+// butterfly layers of the encode (block IFFTs + XOR-accumulate + FFT) or the
+// decode (scale, IFFT, formal derivative, FFT, reveal) in shared memory.  HBM
+// is touched once per shard: algorithmic bytes = (k + p) * size for encode,
+// (present + written) * size for decode.
+//
+// Multiplication by a constant log value lm uses nibble product tables
+// (4 x 16 u16 per lm for GF(2^16), 8 MB in global memory, L1/L2 resident;
+// 2 x 16 bytes per lm for GF(2^8), 8 KB in shared memory).  Butterfly groups
+// are warp-uniform, so a warp's table reads hit one 32-byte sector.
+#include <algorithm>
+#include <cstring>
+
+#include "leo_host.h"
 #include "rsgpu_internal.h"
 
 namespace rsgpu {
+
+constexpr int kLeoThreads = 256;
+constexpr int kLeoTile = 64;          // bytes of every row owned by one CTA
+constexpr int kLeoMaxShards = 2048;   // shard pointers carried in kernel parameters
+constexpr int kLeoMaxRows = 2048;     // rows held in shared memory (2048 * 64 B = 128 KB)
+
+// Per-device tables (built once per context on first use).
+struct LeoState {
+    int device = -1;
+    uint16_t *skew16 = nullptr;  // fftSkew, 65535 entries
+    uint16_t *t16 = nullptr;     // [65536][4][16] nibble products
+    uint16_t *skew8 = nullptr;   // fftSkew8, 255 entries (widened)
+    uint8_t *t8 = nullptr;       // [256][2][16] nibble products
+    ErrLocCache errlocs;
+    ~LeoState() {
+        if (device >= 0) {
+            cudaFree(skew16);
+            cudaFree(t16);
+            cudaFree(skew8);
+            cudaFree(t8);
+        }
+    }
+};
+
+namespace {
+
+struct LeoEncArgs {
+    const uint8_t *shard[kLeoMaxShards];  // k data then p parity pointers
+    int k, p, m;
+    long long size;
+    const uint16_t *skew;
+    const uint16_t *t16;
+    const uint8_t *t8;
+};
+
+struct LeoDecArgs {
+    const uint8_t *shard[kLeoMaxShards];
+    uint16_t errloc[kLeoMaxRows];         // the first n error locators
+    uint32_t present[kLeoMaxShards / 32];
+    uint32_t write[kLeoMaxShards / 32];   // missing shards to reveal
+    int k, p, m, n, input_count;
+    long long size;
+    const uint16_t *skew;
+    const uint16_t *t16;
+    const uint8_t *t8;
+};
+
+__device__ __forceinline__ bool bit(const uint32_t *v, int i) { return (v[i >> 5] >> (i & 31)) & 1u; }
+
+// ---- field policies -----------------------------------------------------
+struct F16 {
+    static constexpr unsigned kMod = 65535;
+    static constexpr int kSyms = 32;  // symbols per 64-byte row tile
+    static __device__ __forceinline__ uint32_t load(const uint8_t *row, int s) {
+        return (uint32_t)row[s] | ((uint32_t)row[32 + s] << 8);
+    }
+    static __device__ __forceinline__ void store(uint8_t *row, int s, uint32_t v) {
+        row[s] = (uint8_t)v;
+        row[32 + s] = (uint8_t)(v >> 8);
+    }
+    const uint16_t *t;
+    __device__ __forceinline__ uint32_t mul(uint32_t x, uint32_t lm) const {
+        const uint16_t *T = t + (size_t)lm * 64;
+        return (uint32_t)__ldg(T + (x & 15)) ^ __ldg(T + 16 + ((x >> 4) & 15)) ^
+               __ldg(T + 32 + ((x >> 8) & 15)) ^ __ldg(T + 48 + (x >> 12));
+    }
+};
+
+struct F8 {
+    static constexpr unsigned kMod = 255;
+    static constexpr int kSyms = 64;
+    static __device__ __forceinline__ uint32_t load(const uint8_t *row, int s) { return row[s]; }
+    static __device__ __forceinline__ void store(uint8_t *row, int s, uint32_t v) { row[s] = (uint8_t)v; }
+    const uint8_t *t;  // shared copy of the 8 KB table
+    __device__ __forceinline__ uint32_t mul(uint32_t x, uint32_t lm) const {
+        const uint8_t *T = t + lm * 32;
+        return (uint32_t)T[x & 15] ^ T[16 + (x >> 4)];
+    }
+};
+
+// Butterflies (galois_noasm.go:94-112; a log multiplier equal to the modulus
+// stands for multiplication by zero and reduces the butterfly to an XOR).
+template <class F>
+__device__ __forceinline__ void fft2(const F &f, uint32_t &x, uint32_t &y, uint32_t lm) {
+    if (lm != F::kMod) x ^= f.mul(y, lm);
+    y ^= x;
+}
+template <class F>
+__device__ __forceinline__ void ifft2(const F &f, uint32_t &x, uint32_t &y, uint32_t lm) {
+    y ^= x;
+    if (lm != F::kMod) x ^= f.mul(y, lm);
+}
+
+// IFFT with decimation in time (ifftDITEncoder leopard.go:764-873 with
+// skew_off = m-1+block*m, ifftDITDecoder :650-693 with skew_off = -1): the
+// layer multipliers are skew[skew_off + iend], [+dist], [+2*dist].
+template <class F>
+__device__ void ifft_rows(const F &f, uint8_t *w, unsigned mtrunc, unsigned m, const uint16_t *skew,
+                          int skew_off) {
+    unsigned dist = 1, dist4 = 4;
+    for (; dist4 <= m; dist = dist4, dist4 <<= 2) {
+        const unsigned groups = (mtrunc + dist4 - 1) / dist4;
+        const unsigned items = groups * dist * F::kSyms;
+        for (unsigned it = threadIdx.x; it < items; it += blockDim.x) {
+            const unsigned q = it / F::kSyms, s = it % F::kSyms;
+            const unsigned r = (q / dist) * dist4, i = r + (q % dist), iend = r + dist;
+            const uint32_t m01 = skew[skew_off + (int)iend];
+            const uint32_t m02 = skew[skew_off + (int)(iend + dist)];
+            const uint32_t m23 = skew[skew_off + (int)(iend + 2 * dist)];
+            uint8_t *p0 = w + (size_t)i * kLeoTile;
+            uint8_t *p1 = p0 + (size_t)dist * kLeoTile, *p2 = p1 + (size_t)dist * kLeoTile,
+                    *p3 = p2 + (size_t)dist * kLeoTile;
+            uint32_t x0 = F::load(p0, s), x1 = F::load(p1, s), x2 = F::load(p2, s), x3 = F::load(p3, s);
+            ifft2(f, x0, x1, m01);
+            ifft2(f, x2, x3, m23);
+            ifft2(f, x0, x2, m02);
+            ifft2(f, x1, x3, m02);
+            F::store(p0, s, x0);
+            F::store(p1, s, x1);
+            F::store(p2, s, x2);
+            F::store(p3, s, x3);
+        }
+        __syncthreads();
+    }
+    if (dist < m) {  // one radix-2 layer left (dist == m / 2)
+        const uint32_t lm = skew[skew_off + (int)dist];
+        const unsigned items = dist * F::kSyms;
+        for (unsigned it = threadIdx.x; it < items; it += blockDim.x) {
+            const unsigned i = it / F::kSyms, s = it % F::kSyms;
+            uint8_t *p0 = w + (size_t)i * kLeoTile, *p1 = p0 + (size_t)dist * kLeoTile;
+            uint32_t x = F::load(p0, s), y = F::load(p1, s);
+            ifft2(f, x, y, lm);
+            F::store(p0, s, x);
+            F::store(p1, s, y);
+        }
+        __syncthreads();
+    }
+}
+
+// FFT with decimation in time (fftDIT leopard.go:696-736): multipliers
+// skew[iend-1], [iend+dist-1], [iend+2*dist-1]; groups start below mtrunc.
+template <class F>
+__device__ void fft_rows(const F &f, uint8_t *w, unsigned mtrunc, unsigned m, const uint16_t *skew) {
+    unsigned dist4 = m, dist = m >> 2;
+    for (; dist != 0; dist4 = dist, dist >>= 2) {
+        const unsigned groups = (mtrunc + dist4 - 1) / dist4;
+        const unsigned items = groups * dist * F::kSyms;
+        for (unsigned it = threadIdx.x; it < items; it += blockDim.x) {
+            const unsigned q = it / F::kSyms, s = it % F::kSyms;
+            const unsigned r = (q / dist) * dist4, i = r + (q % dist), iend = r + dist;
+            const uint32_t m01 = skew[iend - 1], m02 = skew[iend + dist - 1], m23 = skew[iend + 2 * dist - 1];
+            uint8_t *p0 = w + (size_t)i * kLeoTile;
+            uint8_t *p1 = p0 + (size_t)dist * kLeoTile, *p2 = p1 + (size_t)dist * kLeoTile,
+                    *p3 = p2 + (size_t)dist * kLeoTile;
+            uint32_t x0 = F::load(p0, s), x1 = F::load(p1, s), x2 = F::load(p2, s), x3 = F::load(p3, s);
+            fft2(f, x0, x2, m02);
+            fft2(f, x1, x3, m02);
+            fft2(f, x0, x1, m01);
+            fft2(f, x2, x3, m23);
+            F::store(p0, s, x0);
+            F::store(p1, s, x1);
+            F::store(p2, s, x2);
+            F::store(p3, s, x3);
+        }
+        __syncthreads();
+    }
+    if (dist4 == 2) {
+        const unsigned items = ((mtrunc + 1) / 2) * F::kSyms;
+        for (unsigned it = threadIdx.x; it < items; it += blockDim.x) {
+            const unsigned r = 2 * (it / F::kSyms), s = it % F::kSyms;
+            const uint32_t lm = skew[r];
+            uint8_t *p0 = w + (size_t)r * kLeoTile, *p1 = p0 + kLeoTile;
+            uint32_t x = F::load(p0, s), y = F::load(p1, s);
+            fft2(f, x, y, lm);
+            F::store(p0, s, x);
+            F::store(p1, s, y);
+        }
+        __syncthreads();
+    }
+}
+
+// Copies rows [first, first+cnt) of the shard list into w rows [0, cnt) and
+// zero-fills rows [cnt, rows).  16-byte vectors, 4 per row.
+__device__ void load_rows(uint8_t *w, const uint8_t *const *shard, int first, int cnt, int rows, long long off) {
+    for (int v = threadIdx.x; v < rows * 4; v += blockDim.x) {
+        const int r = v >> 2, c = v & 3;
+        uint4 x = make_uint4(0, 0, 0, 0);
+        if (r < cnt) x = __ldcs(reinterpret_cast<const uint4 *>(shard[first + r] + off) + c);
+        reinterpret_cast<uint4 *>(w + (size_t)r * kLeoTile)[c] = x;
+    }
+}
+
+template <class F>
+__device__ void load_tables8(uint8_t *dst, const uint8_t *src) {
+    for (int i = threadIdx.x; i < 256 * 32 / 16; i += blockDim.x)
+        reinterpret_cast<uint4 *>(dst)[i] = reinterpret_cast<const uint4 *>(src)[i];
+}
+
+template <class F>
+__device__ __forceinline__ F make_field(const uint16_t *t16, uint8_t *t8_shared);
+template <>
+__device__ __forceinline__ F16 make_field<F16>(const uint16_t *t16, uint8_t *) { return F16{t16}; }
+template <>
+__device__ __forceinline__ F8 make_field<F8>(const uint16_t *, uint8_t *t8s) { return F8{t8s}; }
+
+constexpr int kT8Bytes = 256 * 32;
+
+// Encode: IFFT of each m-row data block into tmp, XOR-accumulated into acc,
+// then FFT of acc; rows [0, p) of acc are the parity (leopard.go:216-270).
+template <class F>
+__global__ void __launch_bounds__(kLeoThreads) leo_encode_kernel(const __grid_constant__ LeoEncArgs a) {
+    extern __shared__ __align__(16) uint8_t sm[];
+    const bool gf8 = F::kSyms == 64;
+    uint8_t *t8 = sm;
+    uint8_t *acc = sm + (gf8 ? kT8Bytes : 0);
+    const unsigned m = (unsigned)a.m;
+    uint8_t *tmp = acc + (size_t)m * kLeoTile;
+    if (gf8) load_tables8<F>(t8, a.t8);
+    const F f = make_field<F>(a.t16, t8);
+    const long long off = (long long)blockIdx.x * kLeoTile;
+    const int cnt0 = a.k < (int)m ? a.k : (int)m;
+    load_rows(acc, a.shard, 0, cnt0, (int)m, off);
+    __syncthreads();
+    ifft_rows(f, acc, (unsigned)cnt0, m, a.skew, (int)m - 1);
+    for (int b = 1; b * (int)m < a.k; b++) {
+        const int start = b * (int)m;
+        const int cnt = a.k - start < (int)m ? a.k - start : (int)m;
+        load_rows(tmp, a.shard, start, cnt, (int)m, off);
+        __syncthreads();
+        ifft_rows(f, tmp, (unsigned)cnt, m, a.skew, (int)m - 1 + b * (int)m);
+        for (int v = threadIdx.x; v < (int)m * 4; v += blockDim.x)
+            reinterpret_cast<uint4 *>(acc)[v] = make_uint4(
+                reinterpret_cast<uint4 *>(acc)[v].x ^ reinterpret_cast<uint4 *>(tmp)[v].x,
+                reinterpret_cast<uint4 *>(acc)[v].y ^ reinterpret_cast<uint4 *>(tmp)[v].y,
+                reinterpret_cast<uint4 *>(acc)[v].z ^ reinterpret_cast<uint4 *>(tmp)[v].z,
+                reinterpret_cast<uint4 *>(acc)[v].w ^ reinterpret_cast<uint4 *>(tmp)[v].w);
+        __syncthreads();
+    }
+    fft_rows(f, acc, (unsigned)a.p, m, a.skew);
+    for (int v = threadIdx.x; v < a.p * 4; v += blockDim.x) {
+        const int r = v >> 2, c = v & 3;
+        __stcs(reinterpret_cast<uint4 *>(const_cast<uint8_t *>(a.shard[a.k + r]) + off) + c,
+               reinterpret_cast<const uint4 *>(acc + (size_t)r * kLeoTile)[c]);
+    }
+}
+
+// Formal derivative (leopard.go:620-623) on n rows in place.  Row x gains
+// old[x + 2^b] for every b with bit b of x clear and ((x>>b)+1)<<b < n; all
+// reads must see pre-derivative values, and they only reach higher rows, so
+// rows are rewritten in ascending chunks with a barrier between the read
+// and write phase of each chunk.
+__device__ void formal_derivative(uint8_t *w, unsigned n) {
+    const unsigned words_per_row = kLeoTile / 4;
+    const unsigned rows_per_chunk = kLeoThreads / words_per_row;
+    const unsigned x_local = threadIdx.x / words_per_row, word = threadIdx.x % words_per_row;
+    for (unsigned base = 0; base < n; base += rows_per_chunk) {
+        const unsigned x = base + x_local;
+        uint32_t v = 0;
+        if (x < n) {
+            v = reinterpret_cast<const uint32_t *>(w + (size_t)x * kLeoTile)[word];
+            for (unsigned b = 0; (1u << b) < n; b++) {
+                if ((x >> b) & 1u) continue;
+                const unsigned i = ((x >> b) + 1) << b;
+                if (i < n) v ^= reinterpret_cast<const uint32_t *>(w + (size_t)(x + (1u << b)) * kLeoTile)[word];
+            }
+        }
+        __syncthreads();
+        if (x < n) reinterpret_cast<uint32_t *>(w + (size_t)x * kLeoTile)[word] = v;
+        __syncthreads();
+    }
+}
+
+// Decode (leopard.go:582-647 / leopard8.go:536-631).
+template <class F>
+__global__ void __launch_bounds__(kLeoThreads) leo_decode_kernel(const __grid_constant__ LeoDecArgs a) {
+    extern __shared__ __align__(16) uint8_t sm[];
+    const bool gf8 = F::kSyms == 64;
+    uint8_t *t8 = sm;
+    uint8_t *w = sm + (gf8 ? kT8Bytes : 0);
+    if (gf8) load_tables8<F>(t8, a.t8);
+    __syncthreads();
+    const F f = make_field<F>(a.t16, t8);
+    const long long off = (long long)blockIdx.x * kLeoTile;
+    const unsigned n = (unsigned)a.n, m = (unsigned)a.m;
+    // work <- received symbols scaled by their error locators; zeros elsewhere
+    for (unsigned it = threadIdx.x; it < n * F::kSyms; it += blockDim.x) {
+        const unsigned r = it / F::kSyms, s = it % F::kSyms;
+        int src = -1;
+        if (r < (unsigned)a.p) src = a.k + (int)r;
+        else if (r >= m && r < m + (unsigned)a.k) src = (int)(r - m);
+        uint32_t v = 0;
+        if (src >= 0 && bit(a.present, src)) v = f.mul(F::load(a.shard[src] + off, s), a.errloc[r]);
+        F::store(w + (size_t)r * kLeoTile, s, v);
+    }
+    __syncthreads();
+    ifft_rows(f, w, (unsigned)a.input_count, n, a.skew, -1);
+    formal_derivative(w, n);
+    fft_rows(f, w, m + (unsigned)a.k, n, a.skew);
+    // reveal: out = work * (modulus - errloc)
+    for (int i = 0; i < a.k + a.p; i++) {
+        if (!bit(a.write, i)) continue;
+        const unsigned row = i >= a.k ? (unsigned)(i - a.k) : (unsigned)i + m;
+        const uint32_t lm = F::kMod - a.errloc[row];
+        uint8_t *dst = const_cast<uint8_t *>(a.shard[i]) + off;
+        for (int s = threadIdx.x; s < F::kSyms; s += blockDim.x)
+            F::store(dst, s, f.mul(F::load(w + (size_t)row * kLeoTile, s), lm));
+    }
+}
+
+// Builds [65536][4][16] nibble products: mulLog(e << 4q, lm).
+__global__ void build_t16(uint16_t *t, const uint16_t *log, const uint16_t *exp) {
+    for (unsigned idx = blockIdx.x * blockDim.x + threadIdx.x; idx < 65536u * 64u; idx += gridDim.x * blockDim.x) {
+        const unsigned lm = idx >> 6, q = (idx >> 4) & 3, e = idx & 15;
+        const unsigned x = e << (4 * q);
+        uint16_t v = 0;
+        if (x) {
+            unsigned s = (unsigned)log[x] + lm;
+            s = (s + (s >> 16)) & 0xFFFF;  // addMod partial reduction (leopard.go:1001-1006)
+            v = exp[s];
+        }
+        t[idx] = v;
+    }
+}
+
+int ensure_tables(rsgpu_encoder *enc) {
+    rsgpu_ctx *ctx = enc->ctx;
+    if (enc->leo && enc->leo->device == ctx->device) return RS_OK;
+    if (ctx->leo) {
+        enc->leo = ctx->leo;
+        return RS_OK;
+    }
+    auto st = std::make_shared<LeoState>();
+    st->device = ctx->device;
+    const Leo16 &f16 = Leo16::get();
+    const Leo8 &f8 = Leo8::get();
+    RS_CUDA(cudaMalloc(&st->skew16, 65535 * 2));
+    RS_CUDA(cudaMalloc(&st->t16, 65536ull * 64 * 2));
+    RS_CUDA(cudaMalloc(&st->skew8, 255 * 2));
+    RS_CUDA(cudaMalloc(&st->t8, kT8Bytes));
+    RS_CUDA(cudaMemcpy(st->skew16, f16.skew.data(), 65535 * 2, cudaMemcpyHostToDevice));
+    RS_CUDA(cudaMemcpy(st->skew8, f8.skew.data(), 255 * 2, cudaMemcpyHostToDevice));
+    std::vector<uint8_t> t8(kT8Bytes);
+    for (unsigned lm = 0; lm < 256; lm++)
+        for (unsigned q = 0; q < 2; q++)
+            for (unsigned e = 0; e < 16; e++) t8[lm * 32 + q * 16 + e] = (uint8_t)f8.mul_log((uint16_t)(e << (4 * q)), (uint16_t)lm);
+    RS_CUDA(cudaMemcpy(st->t8, t8.data(), kT8Bytes, cudaMemcpyHostToDevice));
+    uint16_t *dlog = nullptr, *dexp = nullptr;
+    RS_CUDA(cudaMalloc(&dlog, 65536 * 2));
+    RS_CUDA(cudaMalloc(&dexp, 65536 * 2));
+    RS_CUDA(cudaMemcpy(dlog, f16.log.data(), 65536 * 2, cudaMemcpyHostToDevice));
+    RS_CUDA(cudaMemcpy(dexp, f16.exp.data(), 65536 * 2, cudaMemcpyHostToDevice));
+    build_t16<<<1024, 256, 0, ctx->stream>>>(st->t16, dlog, dexp);
+    RS_CUDA(cudaGetLastError());
+    RS_CUDA(cudaStreamSynchronize(ctx->stream));
+    cudaFree(dlog);
+    cudaFree(dexp);
+    ctx->leo = st;
+    enc->leo = st;
+    return RS_OK;
+}
+
+bool is16(const rsgpu_encoder *enc) { return enc->codec == RS_CODEC_LEOPARD16; }
+
+// Largest skew index the encoder reads must stay inside fftSkew (the
+// reference indexes past it otherwise, leopard8.go:151,201-233).
+bool encode_fits(const rsgpu_encoder *enc) {
+    const unsigned m = ceil_pow2((unsigned)enc->p);
+    const unsigned blocks = ((unsigned)enc->k + m - 1) / m;
+    const unsigned max_index = (m - 1) + (blocks - 1) * m + (m - 1);
+    return max_index < (is16(enc) ? 65535u : 255u);
+}
+
+template <class K>
+int set_smem(K kern, size_t bytes) {
+    RS_CUDA(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    return RS_OK;
+}
+
+}  // namespace
+
 int leo_create(rsgpu_encoder *enc) {
     if (enc->k <= 0 || enc->p <= 0) return RS_ERR_INV_SHARD_NUM;
     if (enc->k + enc->p > 65536) return RS_ERR_MAX_SHARD_NUM;
+    if (!is16(enc) && ceil_pow2((unsigned)enc->p) + (unsigned)enc->k > 256) return RS_ERR_MAX_SHARD_NUM;
+    if (!encode_fits(enc)) return RS_ERR_MAX_SHARD_NUM;
     return RS_OK;
 }
-int leo_encode(rsgpu_encoder *, uint8_t *const *, size_t) { return RS_ERR_NOT_SUPPORTED; }
-int leo_verify(rsgpu_encoder *, uint8_t *const *, size_t, int *) { return RS_ERR_NOT_SUPPORTED; }
-int leo_reconstruct(rsgpu_encoder *, uint8_t **, const uint8_t *, size_t, int, uint8_t *) {
-    return RS_ERR_NOT_SUPPORTED;
+
+int leo_encode_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, size_t size) {
+    if (size % 64) return RS_ERR_INVALID_SHARD_SIZE;
+    const unsigned m = ceil_pow2((unsigned)enc->p);
+    if (enc->total > kLeoMaxShards || 2 * m > kLeoMaxRows) {
+        set_error("leopard encode: geometry exceeds the shared-memory transform (k+p <= 2048, 2*ceilPow2(p) <= 2048)");
+        return RS_ERR_NOT_SUPPORTED;
+    }
+    int rc = ensure_tables(enc);
+    if (rc) return rc;
+    LeoEncArgs a;
+    memset(&a, 0, sizeof a);
+    for (int i = 0; i < enc->total; i++) a.shard[i] = shards[i];
+    a.k = enc->k;
+    a.p = enc->p;
+    a.m = (int)m;
+    a.size = (long long)size;
+    const bool g16 = is16(enc);
+    a.skew = g16 ? enc->leo->skew16 : enc->leo->skew8;
+    a.t16 = enc->leo->t16;
+    a.t8 = enc->leo->t8;
+    const size_t smem = (size_t)2 * m * kLeoTile + (g16 ? 0 : kT8Bytes);
+    const int grid = (int)(size / kLeoTile);
+    rsgpu_ctx *ctx = enc->ctx;
+    if (g16) {
+        rc = set_smem(leo_encode_kernel<F16>, smem);
+        if (rc) return rc;
+        leo_encode_kernel<F16><<<grid, kLeoThreads, smem, ctx->stream>>>(a);
+    } else {
+        rc = set_smem(leo_encode_kernel<F8>, smem);
+        if (rc) return rc;
+        leo_encode_kernel<F8><<<grid, kLeoThreads, smem, ctx->stream>>>(a);
+    }
+    RS_CUDA(cudaGetLastError());
+    return RS_OK;
 }
-}  // namespace rsgpu
-namespace rsgpu {
-int leo_encode_enqueue(rsgpu_encoder *, uint8_t *const *, size_t) { return RS_ERR_NOT_SUPPORTED; }
-int leo_reconstruct_enqueue(rsgpu_encoder *, uint8_t *const *, const uint8_t *, size_t, int) {
-    return RS_ERR_NOT_SUPPORTED;
+
+int leo_encode(rsgpu_encoder *enc, uint8_t *const *shards, size_t size) {
+    int rc = leo_encode_enqueue(enc, shards, size);
+    if (rc) return rc;
+    RS_CUDA(cudaStreamSynchronize(enc->ctx->stream));
+    return RS_OK;
 }
+
+// Checks of leopard.go:421-460 shared by the device and host entry points.
+static int decode_checks(rsgpu_encoder *enc, const uint8_t *present, size_t size, int recover_all,
+                         bool *nothing) {
+    int np = 0, dp = 0;
+    for (int i = 0; i < enc->total; i++)
+        if (present[i]) {
+            np++;
+            if (i < enc->k) dp++;
+        }
+    *nothing = false;
+    if (np == 0 || size == 0) return RS_ERR_SHARD_NO_DATA;
+    if (np == enc->total || (!recover_all && dp == enc->k)) {
+        *nothing = true;
+        return RS_OK;
+    }
+    if (np < enc->k) return RS_ERR_TOO_FEW_SHARDS;
+    if (size % 64) return RS_ERR_INVALID_SHARD_SIZE;
+    return RS_OK;
+}
+
+int leo_reconstruct_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, const uint8_t *present,
+                            size_t size, int recover_all) {
+    bool nothing = false;
+    int rc = decode_checks(enc, present, size, recover_all, &nothing);
+    if (rc || nothing) return rc;
+    const int k = enc->k, p = enc->p;
+    const unsigned m = ceil_pow2((unsigned)p), n = ceil_pow2(m + (unsigned)k);
+    if (enc->total > kLeoMaxShards || n > kLeoMaxRows) {
+        set_error("leopard decode: geometry exceeds the shared-memory transform (ceilPow2(ceilPow2(p)+k) <= 2048)");
+        return RS_ERR_NOT_SUPPORTED;
+    }
+    rc = ensure_tables(enc);
+    if (rc) return rc;
+    const bool g16 = is16(enc);
+    auto el = enc->leo->errlocs.get(g16 ? 16 : 8, k, p, present);
+    static_assert(sizeof(LeoDecArgs) < 32000, "kernel parameter limit");
+    auto a = std::unique_ptr<LeoDecArgs>(new LeoDecArgs());
+    memset(a.get(), 0, sizeof *a);
+    int input_count = p;
+    for (int i = 0; i < k; i++)
+        if (present[i]) input_count = (int)m + i + 1;
+    const int end = recover_all ? enc->total : k;
+    for (int i = 0; i < enc->total; i++) {
+        a->shard[i] = shards[i];
+        if (present[i]) a->present[i >> 5] |= 1u << (i & 31);
+        else if (i < end) {
+            if (!shards[i]) return RS_ERR_INVALID_INPUT;
+            a->write[i >> 5] |= 1u << (i & 31);
+        }
+    }
+    for (unsigned r = 0; r < n; r++) a->errloc[r] = (*el)[r];
+    a->k = k;
+    a->p = p;
+    a->m = (int)m;
+    a->n = (int)n;
+    a->input_count = input_count;
+    a->size = (long long)size;
+    a->skew = g16 ? enc->leo->skew16 : enc->leo->skew8;
+    a->t16 = enc->leo->t16;
+    a->t8 = enc->leo->t8;
+    const size_t smem = (size_t)n * kLeoTile + (g16 ? 0 : kT8Bytes);
+    const int grid = (int)(size / kLeoTile);
+    rsgpu_ctx *ctx = enc->ctx;
+    if (g16) {
+        rc = set_smem(leo_decode_kernel<F16>, smem);
+        if (rc) return rc;
+        leo_decode_kernel<F16><<<grid, kLeoThreads, smem, ctx->stream>>>(*a);
+    } else {
+        rc = set_smem(leo_decode_kernel<F8>, smem);
+        if (rc) return rc;
+        leo_decode_kernel<F8><<<grid, kLeoThreads, smem, ctx->stream>>>(*a);
+    }
+    RS_CUDA(cudaGetLastError());
+    return RS_OK;
+}
+
+int leo_reconstruct(rsgpu_encoder *enc, uint8_t **shards, const uint8_t *present, size_t size,
+                    int recover_all, uint8_t *written) {
+    if (written) memset(written, 0, (size_t)enc->total);
+    bool nothing = false;
+    int rc = decode_checks(enc, present, size, recover_all, &nothing);
+    if (rc || nothing) return rc;
+    const int end = recover_all ? enc->total : enc->k;
+    for (int i = 0; i < enc->total; i++) {
+        if (present[i]) {
+            if (!shards[i]) return RS_ERR_SHARD_SIZE;
+        } else if (i < end && !shards[i]) {  // allocate like leopard.go:528-534
+            void *pnew = nullptr;
+            RS_CUDA(cudaMalloc(&pnew, size));
+            shards[i] = (uint8_t *)pnew;
+        }
+    }
+    rc = leo_reconstruct_enqueue(enc, shards, present, size, recover_all);
+    if (rc) return rc;
+    RS_CUDA(cudaStreamSynchronize(enc->ctx->stream));
+    if (written)
+        for (int i = 0; i < end; i++)
+            if (!present[i]) written[i] = 1;
+    return RS_OK;
+}
+
+// leopard.go:393-419: re-encode into scratch and compare.
+int leo_verify(rsgpu_encoder *enc, uint8_t *const *shards, size_t size, int *ok) {
+    rsgpu_ctx *ctx = enc->ctx;
+    if (size % 64) return RS_ERR_INVALID_SHARD_SIZE;
+    const size_t pitch = (size + 255) & ~(size_t)255;
+    int rc = ctx->scratch.ensure(pitch * (size_t)enc->p);
+    if (rc) return rc;
+    std::vector<uint8_t *> tmp(shards, shards + enc->total);
+    for (int i = 0; i < enc->p; i++) tmp[enc->k + i] = ctx->scratch.ptr + pitch * i;
+    rc = leo_encode_enqueue(enc, tmp.data(), size);
+    if (rc) return rc;
+    RS_CUDA(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
+    const uint8_t one = 1;
+    for (int i = 0; i < enc->p; i++) {
+        const uint8_t *src = tmp[enc->k + i];
+        uint8_t *chk = shards[enc->k + i];
+        RS_CUDA(launch_gf8_matmul(ctx->stream, ctx->info, &one, 1, 1, &src, &chk, size, kModeVerify, ctx->d_flag));
+    }
+    RS_CUDA(cudaMemcpyAsync(ctx->h_flag, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    RS_CUDA(cudaStreamSynchronize(ctx->stream));
+    *ok = (*ctx->h_flag == 0);
+    return RS_OK;
+}
+
 }  // namespace rsgpu

@@ -47,6 +47,7 @@ struct rsgpu_ctx {
     rsgpu::DeviceBuffer scratch;  // verify temporaries, leopard work rows
     rsgpu::DeviceBuffer staging;  // host-path device copies of shards
     std::vector<cudaEvent_t> events;
+    std::shared_ptr<rsgpu::LeoState> leo;  // Leopard tables, built on first use
 };
 
 struct rsgpu_encoder {

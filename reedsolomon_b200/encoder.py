@@ -285,7 +285,12 @@ class Encoder:
         size, dev = self._prep(shards, nilok=True)
         present = [1 if (s is not None and len(s)) else 0 for s in shards]
         n = self.TotalShards()
-        if required is not None:
+        if self.codec != RS_CODEC_CLASSIC:
+            # leopard.go:378-391: all missing data shards are recovered; parity
+            # too for Reconstruct, or ReconstructSome with a full-length required.
+            recover_all = (not data_only) if required is None else len(required) == n
+            want = [not present[i] and (i < self._k or recover_all) for i in range(n)]
+        elif required is not None:
             req = [bool(r) for r in required]
             want = [not present[i] and i < len(req) and req[i] for i in range(n)]
         else:
