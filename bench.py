@@ -47,6 +47,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     ap.add_argument("--shard-mib", type=int, default=SHARD >> 20,
                     help="shard size; the headline workload is 64 MiB")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the secondary measurements (verify, reconstruct, batch, leopard)")
+    ap.add_argument("--batch-stripes", type=int, default=4096)
     ap.add_argument("--variant", type=int, default=-1,
                     help="force one GF(2^8) kernel variant instead of autotuning (profiling runs)")
     return ap.parse_args()
@@ -204,6 +207,154 @@ def run_e2e(args, enc, lib, shards, S, stream, dev, world, barrier):
     return world * k * S / (ems / e2e_steps / 1e3) / 1e9
 
 
+def _ev():
+    import torch
+    return torch.cuda.Event(enable_timing=True)
+
+
+def _pct(xs, q):
+    return float(np.percentile(np.asarray(xs), q)) if xs else None
+
+
+def extra_reconstruct(enc, lib, shards, S, stream, reps=32):
+    """C2: 32 seeded 4-erasure patterns on the RS(10,4) x 64 MiB stripe."""
+    import torch
+    import reedsolomon_b200 as rs
+    k, p = K_DATA, P_PARITY
+    rng = np.random.default_rng(2024)
+    combos = [tuple(sorted(rng.choice(k + p, size=4, replace=False).tolist())) for _ in range(reps)]
+    out = {}
+    for data_only in (0, 1):
+        lat, gbs = [], []
+        for lost in combos:
+            present = [0 if i in lost else 1 for i in range(k + p)]
+            pres = rs._lib.u8_array(present)
+            ptrs = rs._lib.ptr_array([s.data_ptr() for s in shards])  # outputs overwrite erased shards in place
+            n_out = sum(1 for i in lost if i < k or not data_only)
+            a, b = _ev(), _ev()
+            a.record(stream)
+            rs.encoder.check(lib.rsgpu_reconstruct_async(enc._h, ptrs, pres, S, data_only))
+            b.record(stream)
+            b.synchronize()
+            ms = a.elapsed_time(b)
+            lat.append(ms)
+            gbs.append(k * S / (ms / 1e3) / 1e9)
+            _ = n_out
+        key = "reconstruct_data" if data_only else "reconstruct"
+        out[key] = {"patterns": reps, "erasures": 4, "data_GBps_median": round(_pct(gbs, 50), 1),
+                    "latency_ms_p50": round(_pct(lat, 50), 4), "latency_ms_p99": round(_pct(lat, 99), 4)}
+    return out
+
+
+def extra_verify(enc, shards, steps=10):
+    import torch
+    a, b = _ev(), _ev()
+    stream = torch.cuda.current_stream()
+    ok = True
+    a.record(stream)
+    for _ in range(steps):
+        ok &= enc.Verify(shards)
+    b.record(stream)
+    b.synchronize()
+    ms = a.elapsed_time(b) / steps
+    return {"ok": bool(ok), "ms": round(ms, 4), "data_GBps": round(K_DATA * len(shards[0]) / (ms / 1e3) / 1e9, 1)}
+
+
+def extra_batch(dev, n_stripes, seed=77):
+    """C3: n stripes, k~U[4,32], p~U[2,8], shard size log-uniform 4 KiB..1 MiB (64 B multiple),
+    erasures ~U[1,p]: all encodes then all reconstructs, persistent vs per-stripe vs graph."""
+    import torch
+    import reedsolomon_b200 as rs
+    rng = np.random.default_rng(seed)
+    geo = []
+    total = 0
+    for _ in range(n_stripes):
+        k = int(rng.integers(4, 33))
+        p = int(rng.integers(2, 9))
+        size = max(64, int(np.exp(rng.uniform(np.log(4096), np.log(1 << 20)))) // 64 * 64)
+        e = int(rng.integers(1, p + 1))
+        lost = sorted(rng.choice(k + p, size=e, replace=False).tolist())
+        geo.append((k, p, size, lost))
+        total += (k + p) * ((size + 255) // 256 * 256)
+    pool = torch.empty(total, dtype=torch.uint8, device=dev)
+    g = torch.Generator(device=dev).manual_seed(seed)
+    off = 0
+    enc_b, rec_b = rs.Batch(), rs.Batch()
+    for (k, p, size, lost) in geo:
+        pitch = (size + 255) // 256 * 256
+        sh = [pool[off + i * pitch: off + i * pitch + size] for i in range(k + p)]
+        off += (k + p) * pitch
+        for i in range(k):
+            sh[i].copy_(torch.randint(0, 256, (size,), dtype=torch.uint8, device=dev, generator=g))
+        enc_b.add_encode(k, p, sh)
+        present = [0 if i in lost else 1 for i in range(k + p)]
+        rec_b.add_reconstruct(k, p, sh, present)
+    ie, ir = enc_b.info(), rec_b.info()
+    res = {"stripes": n_stripes, "encode_jobs": ie["jobs"], "reconstruct_jobs": ir["jobs"],
+           "bytes_per_pass": ie["bytes"] + ir["bytes"]}
+    stream = torch.cuda.current_stream(dev)
+    for mode in ("persistent", "graph", "per_stripe"):
+        enc_b.run(mode)
+        rec_b.run(mode)
+        times = []
+        for _ in range(3):
+            a, b = _ev(), _ev()
+            a.record(stream)
+            enc_b.run(mode, wait=False)
+            rec_b.run(mode, wait=False)
+            b.record(stream)
+            b.synchronize()
+            times.append(a.elapsed_time(b))
+        ms = min(times)
+        res[mode] = {"ms": round(ms, 3), "GBps": round(res["bytes_per_pass"] / (ms / 1e3) / 1e9, 1)}
+    res["speedup_persistent_vs_per_stripe"] = round(res["per_stripe"]["ms"] / res["persistent"]["ms"], 2)
+    res["speedup_persistent_vs_graph"] = round(res["graph"]["ms"] / res["persistent"]["ms"], 2)
+    del pool
+    return res
+
+
+def extra_leopard(dev):
+    """C4: Leopard GF(2^16) 1000+200 x 64 KiB and GF(2^8) 192+56 x 256 KiB encode / reconstruct."""
+    import torch
+    import reedsolomon_b200 as rs
+    out = {}
+    for name, gf, k, p, size in (("leopard16_1000+200x64KiB", 16, 1000, 200, 65536),
+                                 ("leopard8_192+56x256KiB", 8, 192, 56, 262144)):
+        g = torch.Generator(device=dev).manual_seed(k + p)
+        sh = [torch.randint(0, 256, (size,), dtype=torch.uint8, device=dev, generator=g) for _ in range(k)]
+        sh += [torch.empty(size, dtype=torch.uint8, device=dev) for _ in range(p)]
+        enc = rs.New(k, p, rs.WithLeopardGF16() if gf == 16 else rs.WithLeopardGF())
+        enc.Encode(sh)
+        stream = torch.cuda.current_stream(dev)
+        lib = rs.lib()
+        ptrs = rs._lib.ptr_array([s.data_ptr() for s in sh])
+        reps = 5
+        a, b = _ev(), _ev()
+        a.record(stream)
+        for _ in range(reps):
+            rs.encoder.check(lib.rsgpu_encode_async(enc._h, ptrs, size))
+        b.record(stream)
+        b.synchronize()
+        ms_e = a.elapsed_time(b) / reps
+        rng = np.random.default_rng(gf)
+        lost = sorted(rng.choice(k + p, size=p, replace=False).tolist())
+        present = rs._lib.u8_array([0 if i in lost else 1 for i in range(k + p)])
+        rs.encoder.check(lib.rsgpu_reconstruct_async(enc._h, ptrs, present, size, 0))  # warm (error locators)
+        a, b = _ev(), _ev()
+        a.record(stream)
+        for _ in range(reps):
+            rs.encoder.check(lib.rsgpu_reconstruct_async(enc._h, ptrs, present, size, 0))
+        b.record(stream)
+        b.synchronize()
+        ms_r = a.elapsed_time(b) / reps
+        assert enc.Verify(sh)
+        out[name] = {"encode_ms": round(ms_e, 4), "encode_data_GBps": round(k * size / (ms_e / 1e3) / 1e9, 1),
+                     "encode_frac_of_hbm": round((k + p) * size / (ms_e / 1e3) / 1e9 / peaks()[0], 4),
+                     "reconstruct_ms": round(ms_r, 4), "erasures": p,
+                     "reconstruct_data_GBps": round(k * size / (ms_r / 1e3) / 1e9, 1)}
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -277,6 +428,12 @@ def run_ours(args):
     if not args.no_e2e:
         e2e = run_e2e(args, enc, lib, shards, S, stream, dev, world, barrier)
 
+    extras = None
+    if not args.no_extras:
+        extras = {"verify": extra_verify(enc, shards)}
+        extras.update(extra_reconstruct(enc, lib, shards, S, stream))
+        extras["batch"] = extra_batch(dev, args.batch_stripes)
+        extras["leopard"] = extra_leopard(dev)
     out = None
     if rank == 0:
         out = {
@@ -297,6 +454,7 @@ def run_ours(args):
                 "d2h_bytes_per_step": p * S, "path": "rsgpu_encode_host, pinned host buffers"},
             "gpu_launches": args.steps,
             "autotune": tuning,
+            "extras": extras,
             "clocks": clk.summary(),
         }
         if not args.no_cpu_baseline:

@@ -180,6 +180,43 @@ int rsgpu_gal_mul_slice(rsgpu_ctx *ctx, uint8_t c, const uint8_t *in, uint8_t *o
 /* sliceXor (galois_amd64.go:162-203): out ^= in */
 int rsgpu_slice_xor(rsgpu_ctx *ctx, const uint8_t *in, uint8_t *out, size_t n);
 
+/* ---- batched execution (no counterpart in the reference, which runs one
+ * Encode / Reconstruct / Verify call per stripe: reedsolomon.go:686,1670,857) */
+#define RS_JOB_ENCODE 0
+#define RS_JOB_RECONSTRUCT 1
+#define RS_JOB_RECONSTRUCT_DATA 2
+#define RS_JOB_VERIFY 3
+
+#define RS_BATCH_PERSISTENT 0 /* one launch over every job's tiles */
+#define RS_BATCH_PER_STRIPE 1 /* one launch per stripe operation (baseline) */
+#define RS_BATCH_GRAPH 2      /* the per-stripe launches captured once in a CUDA graph */
+
+typedef struct rsgpu_stripe {
+    int op;                   /* RS_JOB_* */
+    int data_shards, parity_shards;
+    size_t shard_size;
+    uint8_t *const *shards;   /* k+p device pointers; reconstruct outputs preallocated */
+    const uint8_t *present;   /* reconstruct: k+p flags, 0 = missing */
+} rsgpu_stripe;
+
+typedef struct rsgpu_batch rsgpu_batch;
+/* A batch of classic-codec stripe operations (k <= 32 per stripe), each
+ * stripe with its own geometry, size and erasure set. */
+int rsgpu_batch_create(rsgpu_ctx *ctx, const rsgpu_options *opts, rsgpu_batch **out);
+int rsgpu_batch_destroy(rsgpu_batch *batch);
+int rsgpu_batch_clear(rsgpu_batch *batch);
+/* Plans stripes on the host (matrices, decode rows via the inversion tree). */
+int rsgpu_batch_add(rsgpu_batch *batch, const rsgpu_stripe *stripes, int n);
+/* Runs all planned jobs on the context stream (RS_BATCH_*); _run waits. */
+int rsgpu_batch_run(rsgpu_batch *batch, int mode);
+int rsgpu_batch_run_async(rsgpu_batch *batch, int mode);
+/* Verify outcome per added stripe in add order (1 = parity matches). */
+int rsgpu_batch_results(rsgpu_batch *batch, int *ok, int n);
+/* Stripes, jobs, tiles and algorithmic bytes (reads + writes) of the batch. */
+int rsgpu_batch_info(rsgpu_batch *batch, int *n_stripes, int *n_jobs, long long *n_tiles, double *bytes);
+/* Tile size of the persistent launch in bytes (multiple of 4096; 0 = default). */
+int rsgpu_batch_set_tile(rsgpu_batch *batch, int tile_bytes);
+
 /* ---- autotuner (no counterpart in the reference: CPU dispatch there is by
  * cpuid, galois_gen_switch_amd64.go:29-44) -------------------------------- */
 /* Times every GF(2^8) kernel variant on scratch buffers of the given geometry

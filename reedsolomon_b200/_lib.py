@@ -28,6 +28,17 @@ class RsOptions(ctypes.Structure):
     ]
 
 
+class RsStripe(ctypes.Structure):
+    _fields_ = [
+        ("op", c_int),
+        ("data_shards", c_int),
+        ("parity_shards", c_int),
+        ("shard_size", c_size),
+        ("shards", c_voidp),
+        ("present", c_voidp),
+    ]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "rsgpu_ctx_create": (c_int, [c_int, ctypes.POINTER(c_voidp)]),
@@ -66,6 +77,16 @@ SIGNATURES = {
     "rsgpu_autotune_gf8": (c_int, [c_voidp, c_int, c_int, c_size, c_int, c_int, c_voidp, c_intp]),
     "rsgpu_force_variant": (c_int, [c_int]),
     "rsgpu_num_variants": (c_int, []),
+    "rsgpu_batch_create": (c_int, [c_voidp, c_voidp, ctypes.POINTER(c_voidp)]),
+    "rsgpu_batch_destroy": (c_int, [c_voidp]),
+    "rsgpu_batch_clear": (c_int, [c_voidp]),
+    "rsgpu_batch_add": (c_int, [c_voidp, c_voidp, c_int]),
+    "rsgpu_batch_run": (c_int, [c_voidp, c_int]),
+    "rsgpu_batch_run_async": (c_int, [c_voidp, c_int]),
+    "rsgpu_batch_results": (c_int, [c_voidp, c_intp, c_int]),
+    "rsgpu_batch_info": (c_int, [c_voidp, c_intp, c_intp, ctypes.POINTER(ctypes.c_longlong),
+                                 ctypes.POINTER(ctypes.c_double)]),
+    "rsgpu_batch_set_tile": (c_int, [c_voidp, c_int]),
     "rsgpu_build_matrix": (c_int, [c_int, c_int, c_int, c_voidp]),
     "rsgpu_invert_matrix": (c_int, [c_voidp, c_int, c_voidp]),
     "rsgpu_gal_mul": (ctypes.c_uint8, [ctypes.c_uint8, ctypes.c_uint8]),

@@ -419,3 +419,81 @@ def invert_matrix(m):
     out = np.zeros_like(m)
     check(L.lib().rsgpu_invert_matrix(m.ctypes.data, m.shape[0], out.ctypes.data))
     return out
+
+
+# ---- batched mixed-geometry execution ---------------------------------------
+RS_JOB_ENCODE, RS_JOB_RECONSTRUCT, RS_JOB_RECONSTRUCT_DATA, RS_JOB_VERIFY = 0, 1, 2, 3
+BATCH_MODES = {"persistent": 0, "per_stripe": 1, "graph": 2}
+
+
+class Batch:
+    """Many stripe operations of mixed geometry run as one launch.
+
+    add_* plan on the host (matrices, decode rows); run() executes every
+    planned job on the GPU: mode "persistent" (one launch), "per_stripe"
+    (one launch per stripe operation) or "graph" (those launches captured
+    once into a CUDA graph).  Shards are CUDA uint8 tensors; reconstruct
+    outputs must be preallocated tensors, with `present` marking valid shards.
+    """
+
+    def __init__(self, device=0, *opts):
+        self.ctx = Context.get(device)
+        o = {"matrix": "default", "fast_one_parity": 0, "inversion_cache": 1}
+        for f in opts:
+            f(o)
+        ro = L.RsOptions()
+        L.lib().rsgpu_options_init(ctypes.byref(ro))
+        ro.matrix_kind = _MATRIX[o["matrix"]]
+        ro.fast_one_parity = o["fast_one_parity"]
+        ro.inversion_cache = o["inversion_cache"]
+        h = ctypes.c_void_p()
+        check(L.lib().rsgpu_batch_create(self.ctx.handle, ctypes.byref(ro), ctypes.byref(h)))
+        self._h = h
+        self.n = 0
+
+    def __del__(self):
+        try:
+            L.lib().rsgpu_batch_destroy(self._h)
+        except Exception:
+            pass
+
+    def _add(self, op, k, p, shards, present=None):
+        ptrs = L.ptr_array([_ptr(s) for s in shards])
+        st = L.RsStripe(op, k, p, _size(shards), ctypes.cast(ptrs, ctypes.c_void_p),
+                        ctypes.cast(L.u8_array(present), ctypes.c_void_p) if present is not None else None)
+        keep = (ptrs, st)
+        if present is not None:
+            pres = L.u8_array(present)
+            st.present = ctypes.cast(pres, ctypes.c_void_p)
+            keep = keep + (pres,)
+        check(L.lib().rsgpu_batch_add(self._h, ctypes.byref(st), 1))
+        self.n += 1
+        return self.n - 1
+
+    def add_encode(self, k, p, shards):
+        return self._add(RS_JOB_ENCODE, k, p, shards)
+
+    def add_verify(self, k, p, shards):
+        return self._add(RS_JOB_VERIFY, k, p, shards)
+
+    def add_reconstruct(self, k, p, shards, present, data_only=False):
+        return self._add(RS_JOB_RECONSTRUCT_DATA if data_only else RS_JOB_RECONSTRUCT, k, p, shards, present)
+
+    def set_tile(self, tile_bytes):
+        check(L.lib().rsgpu_batch_set_tile(self._h, int(tile_bytes)))
+
+    def run(self, mode="persistent", wait=True):
+        self.ctx.bind_current_stream()
+        f = L.lib().rsgpu_batch_run if wait else L.lib().rsgpu_batch_run_async
+        check(f(self._h, BATCH_MODES[mode]))
+
+    def results(self):
+        ok = (ctypes.c_int * max(1, self.n))()
+        check(L.lib().rsgpu_batch_results(self._h, ok, self.n))
+        return [bool(ok[i]) for i in range(self.n)]
+
+    def info(self):
+        ns, nj = ctypes.c_int(), ctypes.c_int()
+        nt, by = ctypes.c_longlong(), ctypes.c_double()
+        check(L.lib().rsgpu_batch_info(self._h, ctypes.byref(ns), ctypes.byref(nj), ctypes.byref(nt), ctypes.byref(by)))
+        return {"stripes": ns.value, "jobs": nj.value, "tiles": nt.value, "bytes": by.value}
