@@ -99,6 +99,8 @@ int rsgpu_alloc_shards(rsgpu_ctx *ctx, int n, size_t each, uint8_t **out);
 int rsgpu_free(rsgpu_ctx *ctx, void *device_ptr);
 int rsgpu_host_alloc(size_t bytes, void **out); /* pinned host memory */
 int rsgpu_host_free(void *p);
+/* Synchronous copy between any host / device addresses (unified addressing). */
+int rsgpu_memcpy(void *dst, const void *src, size_t bytes);
 
 /* ---- encoder (Encoder / Extensions interfaces, reedsolomon.go:25-165) ----- */
 void rsgpu_options_init(rsgpu_options *opts);
@@ -216,6 +218,60 @@ int rsgpu_batch_results(rsgpu_batch *batch, int *ok, int n);
 int rsgpu_batch_info(rsgpu_batch *batch, int *n_stripes, int *n_jobs, long long *n_tiles, double *bytes);
 /* Tile size of the persistent launch in bytes (multiple of 4096; 0 = default). */
 int rsgpu_batch_set_tile(rsgpu_batch *batch, int tile_bytes);
+
+/* ---- request server (no counterpart in the reference) --------------------
+ * Continuous batching over device-resident stripes: any host thread submits
+ * requests; a server thread admits them in arrival order while the bytes of
+ * work in flight stay under `inflight_budget` and reconstruct outputs without
+ * a caller buffer fit in an HBM arena of `arena_bytes`, and launches each
+ * admitted group as one micro-batch on one of `streams` streams, so requests
+ * arriving while others run are admitted as soon as a stream frees up and
+ * their work overlaps on the device. */
+typedef struct rsgpu_request {
+    int op;                     /* RS_JOB_* (verify: classic stripes only) */
+    int data_shards, parity_shards;
+    int leopard;                /* RS_LEOPARD_* as in rsgpu_options */
+    size_t shard_size;
+    uint8_t **shards;           /* k+p device pointers; NULL reconstruct outputs are
+                                   allocated from the arena and written back here */
+    const uint8_t *present;     /* reconstruct: 0 = missing (NULL = all present) */
+    uint64_t tag;               /* returned in the completion */
+    int result;                 /* verify: set to 1 when parity matches */
+} rsgpu_request;
+
+typedef struct rsgpu_completion {
+    uint64_t ticket, tag;
+    int status;                 /* RS_OK or the request's error */
+    double latency_us;          /* submit -> device completion */
+} rsgpu_completion;
+
+typedef struct rsgpu_server_stats {
+    uint64_t submitted, completed, failed;
+    double bytes;               /* algorithmic bytes of completed requests */
+    double elapsed_s;           /* first submit -> last completion */
+    double p50_us, p99_us, mean_us, max_us;
+    double max_inflight_bytes;
+} rsgpu_server_stats;
+
+typedef struct rsgpu_server rsgpu_server;
+int rsgpu_server_create(rsgpu_ctx *ctx, size_t arena_bytes, size_t inflight_budget, int max_batch,
+                        int streams, rsgpu_server **out);
+/* The request (and its shards array) must stay valid until completion. */
+int rsgpu_server_submit(rsgpu_server *srv, rsgpu_request *req, uint64_t *ticket);
+/* Up to `max` completions, non-blocking; returns how many. */
+int rsgpu_server_poll(rsgpu_server *srv, rsgpu_completion *out, int max);
+/* Frees a completed request's arena outputs and bookkeeping. */
+int rsgpu_server_release(rsgpu_server *srv, uint64_t ticket);
+/* Waits until nothing is queued or running; RS_ERR_TIMEOUT after timeout_ms. */
+int rsgpu_server_wait_idle(rsgpu_server *srv, int timeout_ms);
+int rsgpu_server_get_stats(rsgpu_server *srv, rsgpu_server_stats *out);
+int rsgpu_server_reset_stats(rsgpu_server *srv);
+/* Open-loop load generator: submits reqs[i] at arrival_us[i] microseconds
+ * after the call from a dedicated thread; returns when all are submitted. */
+int rsgpu_server_replay(rsgpu_server *srv, rsgpu_request *reqs, const double *arrival_us, int n,
+                        uint64_t *tickets);
+/* Drains queued and running work, then frees the server. */
+int rsgpu_server_destroy(rsgpu_server *srv);
 
 /* ---- autotuner (no counterpart in the reference: CPU dispatch there is by
  * cpuid, galois_gen_switch_amd64.go:29-44) -------------------------------- */

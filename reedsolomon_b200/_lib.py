@@ -39,6 +39,32 @@ class RsStripe(ctypes.Structure):
     ]
 
 
+class RsRequest(ctypes.Structure):
+    _fields_ = [
+        ("op", c_int),
+        ("data_shards", c_int),
+        ("parity_shards", c_int),
+        ("leopard", c_int),
+        ("shard_size", c_size),
+        ("shards", c_voidp),
+        ("present", c_voidp),
+        ("tag", ctypes.c_uint64),
+        ("result", c_int),
+    ]
+
+
+class RsCompletion(ctypes.Structure):
+    _fields_ = [("ticket", ctypes.c_uint64), ("tag", ctypes.c_uint64), ("status", c_int),
+                ("latency_us", ctypes.c_double)]
+
+
+class RsServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("failed", ctypes.c_uint64),
+                ("bytes", ctypes.c_double), ("elapsed_s", ctypes.c_double), ("p50_us", ctypes.c_double),
+                ("p99_us", ctypes.c_double), ("mean_us", ctypes.c_double), ("max_us", ctypes.c_double),
+                ("max_inflight_bytes", ctypes.c_double)]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "rsgpu_ctx_create": (c_int, [c_int, ctypes.POINTER(c_voidp)]),
@@ -53,6 +79,7 @@ SIGNATURES = {
     "rsgpu_free": (c_int, [c_voidp, c_voidp]),
     "rsgpu_host_alloc": (c_int, [c_size, ctypes.POINTER(c_voidp)]),
     "rsgpu_host_free": (c_int, [c_voidp]),
+    "rsgpu_memcpy": (c_int, [c_voidp, c_voidp, c_size]),
     "rsgpu_options_init": (None, [ctypes.POINTER(RsOptions)]),
     "rsgpu_encoder_new": (c_int, [c_voidp, c_int, c_int, ctypes.POINTER(RsOptions), ctypes.POINTER(c_voidp)]),
     "rsgpu_encoder_free": (c_int, [c_voidp]),
@@ -87,6 +114,15 @@ SIGNATURES = {
     "rsgpu_batch_info": (c_int, [c_voidp, c_intp, c_intp, ctypes.POINTER(ctypes.c_longlong),
                                  ctypes.POINTER(ctypes.c_double)]),
     "rsgpu_batch_set_tile": (c_int, [c_voidp, c_int]),
+    "rsgpu_server_create": (c_int, [c_voidp, c_size, c_size, c_int, c_int, ctypes.POINTER(c_voidp)]),
+    "rsgpu_server_submit": (c_int, [c_voidp, c_voidp, ctypes.POINTER(ctypes.c_uint64)]),
+    "rsgpu_server_poll": (c_int, [c_voidp, c_voidp, c_int]),
+    "rsgpu_server_release": (c_int, [c_voidp, ctypes.c_uint64]),
+    "rsgpu_server_wait_idle": (c_int, [c_voidp, c_int]),
+    "rsgpu_server_get_stats": (c_int, [c_voidp, c_voidp]),
+    "rsgpu_server_reset_stats": (c_int, [c_voidp]),
+    "rsgpu_server_replay": (c_int, [c_voidp, c_voidp, c_voidp, c_int, c_voidp]),
+    "rsgpu_server_destroy": (c_int, [c_voidp]),
     "rsgpu_build_matrix": (c_int, [c_int, c_int, c_int, c_voidp]),
     "rsgpu_invert_matrix": (c_int, [c_voidp, c_int, c_voidp]),
     "rsgpu_gal_mul": (ctypes.c_uint8, [ctypes.c_uint8, ctypes.c_uint8]),

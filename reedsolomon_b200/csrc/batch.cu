@@ -418,26 +418,43 @@ int rsgpu_batch_add(rsgpu_batch *b, const rsgpu_stripe *s, int n) {
 
 int rsgpu_batch_run_async(rsgpu_batch *b, int mode) {
     if (!b) return RS_ERR_INVALID_INPUT;
+    std::lock_guard<std::recursive_mutex> lk(b->ctx->mu);
+    return batch_run_on(b, mode, b->ctx->stream);
+}
+
+}  // extern "C"
+
+int rsgpu::batch_stripe_count(const rsgpu_batch *b) { return b->n_stripes; }
+
+int rsgpu::batch_read_flags(rsgpu_batch *b, int *ok, int n, cudaStream_t st) {
+    if (n <= 0) return RS_OK;
+    std::vector<int> flags(n);
+    RS_CUDA(cudaMemcpyAsync(flags.data(), b->d_flags, n * sizeof(int), cudaMemcpyDeviceToHost, st));
+    RS_CUDA(cudaStreamSynchronize(st));
+    for (int i = 0; i < n; i++) ok[i] = flags[i] == 0;
+    return RS_OK;
+}
+
+int rsgpu::batch_run_on(rsgpu_batch *b, int mode, cudaStream_t st) {
     rsgpu_ctx *ctx = b->ctx;
-    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
     int rc = upload(b);
     if (rc) return rc;
-    RS_CUDA(cudaMemsetAsync(b->d_flags, 0, std::max(1, b->n_stripes) * sizeof(int), ctx->stream));
+    RS_CUDA(cudaMemsetAsync(b->d_flags, 0, std::max(1, b->n_stripes) * sizeof(int), st));
     if (mode == RS_BATCH_PERSISTENT) {
-        rc = launch_persistent(b, ctx->stream);
+        rc = launch_persistent(b, st);
         if (rc) return rc;
-        return launch_per_job(b, ctx->stream, b->irregular);
+        return launch_per_job(b, st, b->irregular);
     }
     if (mode == RS_BATCH_PER_STRIPE) {
-        rc = launch_per_job(b, ctx->stream, b->jobs);
+        rc = launch_per_job(b, st, b->jobs);
         if (rc) return rc;
-        return launch_per_job(b, ctx->stream, b->irregular);
+        return launch_per_job(b, st, b->irregular);
     }
     if (mode == RS_BATCH_GRAPH) {
         if (!b->graph) {
             // capture on the context's own stream, replay on the current one
             cudaStream_t cs = ctx->own_stream;
-            RS_CUDA(cudaStreamSynchronize(ctx->stream));
+            RS_CUDA(cudaStreamSynchronize(st));
             RS_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed));
             int r1 = launch_per_job(b, cs, b->jobs);
             int r2 = r1 ? r1 : launch_per_job(b, cs, b->irregular);
@@ -452,11 +469,13 @@ int rsgpu_batch_run_async(rsgpu_batch *b, int mode) {
             cudaGraphDestroy(g);
             RS_CUDA(e);
         }
-        RS_CUDA(cudaGraphLaunch(b->graph, ctx->stream));
+        RS_CUDA(cudaGraphLaunch(b->graph, st));
         return RS_OK;
     }
     return RS_ERR_INVALID_INPUT;
 }
+
+extern "C" {
 
 int rsgpu_batch_run(rsgpu_batch *b, int mode) {
     int rc = rsgpu_batch_run_async(b, mode);

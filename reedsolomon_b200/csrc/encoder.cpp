@@ -317,6 +317,12 @@ int rsgpu_host_free(void *p) {
     return RS_OK;
 }
 
+int rsgpu_memcpy(void *dst, const void *src, size_t bytes) {
+    if ((!dst || !src) && bytes) return RS_ERR_INVALID_INPUT;
+    if (bytes) RS_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyDefault));
+    return RS_OK;
+}
+
 void rsgpu_options_init(rsgpu_options *o) {
     if (!o) return;
     memset(o, 0, sizeof *o);

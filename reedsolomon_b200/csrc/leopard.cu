@@ -24,7 +24,8 @@
 
 namespace rsgpu {
 
-constexpr int kLeoThreads = 256;
+constexpr int kLeoThreads = 256;        // encode CTAs (2m rows of shared memory each)
+constexpr int kLeoDecodeThreads = 1024; // decode CTAs hold up to 128 KB: one per SM, so 32 warps
 constexpr int kLeoTile = 64;          // bytes of every row owned by one CTA
 constexpr int kLeoMaxShards = 2048;   // shard pointers carried in kernel parameters
 constexpr int kLeoMaxRows = 2048;     // rows held in shared memory (2048 * 64 B = 128 KB)
@@ -122,13 +123,13 @@ __device__ __forceinline__ void ifft2(const F &f, uint32_t &x, uint32_t &y, uint
 template <class F>
 __device__ void ifft_rows(const F &f, uint8_t *w, unsigned mtrunc, unsigned m, const uint16_t *skew,
                           int skew_off) {
-    unsigned dist = 1, dist4 = 4;
-    for (; dist4 <= m; dist = dist4, dist4 <<= 2) {
-        const unsigned groups = (mtrunc + dist4 - 1) / dist4;
-        const unsigned items = groups * dist * F::kSyms;
+    unsigned dist = 1, dist4 = 4, ld = 0;  // dist == 1 << ld
+    for (; dist4 <= m; dist = dist4, dist4 <<= 2, ld += 2) {
+        const unsigned groups = (mtrunc + dist4 - 1) >> (ld + 2);
+        const unsigned items = (groups << ld) * F::kSyms;
         for (unsigned it = threadIdx.x; it < items; it += blockDim.x) {
             const unsigned q = it / F::kSyms, s = it % F::kSyms;
-            const unsigned r = (q / dist) * dist4, i = r + (q % dist), iend = r + dist;
+            const unsigned r = (q >> ld) << (ld + 2), i = r + (q & (dist - 1)), iend = r + dist;
             const uint32_t m01 = skew[skew_off + (int)iend];
             const uint32_t m02 = skew[skew_off + (int)(iend + dist)];
             const uint32_t m23 = skew[skew_off + (int)(iend + 2 * dist)];
@@ -167,12 +168,14 @@ __device__ void ifft_rows(const F &f, uint8_t *w, unsigned mtrunc, unsigned m, c
 template <class F>
 __device__ void fft_rows(const F &f, uint8_t *w, unsigned mtrunc, unsigned m, const uint16_t *skew) {
     unsigned dist4 = m, dist = m >> 2;
-    for (; dist != 0; dist4 = dist, dist >>= 2) {
-        const unsigned groups = (mtrunc + dist4 - 1) / dist4;
-        const unsigned items = groups * dist * F::kSyms;
+    unsigned ld = 0;  // dist == 1 << ld
+    while ((2u << ld) <= dist) ld++;
+    for (; dist != 0; dist4 = dist, dist >>= 2, ld -= 2) {
+        const unsigned groups = (mtrunc + dist4 - 1) >> (ld + 2);
+        const unsigned items = (groups << ld) * F::kSyms;
         for (unsigned it = threadIdx.x; it < items; it += blockDim.x) {
             const unsigned q = it / F::kSyms, s = it % F::kSyms;
-            const unsigned r = (q / dist) * dist4, i = r + (q % dist), iend = r + dist;
+            const unsigned r = (q >> ld) << (ld + 2), i = r + (q & (dist - 1)), iend = r + dist;
             const uint32_t m01 = skew[iend - 1], m02 = skew[iend + dist - 1], m23 = skew[iend + 2 * dist - 1];
             uint8_t *p0 = w + (size_t)i * kLeoTile;
             uint8_t *p1 = p0 + (size_t)dist * kLeoTile, *p2 = p1 + (size_t)dist * kLeoTile,
@@ -276,7 +279,7 @@ __global__ void __launch_bounds__(kLeoThreads) leo_encode_kernel(const __grid_co
 // and write phase of each chunk.
 __device__ void formal_derivative(uint8_t *w, unsigned n) {
     const unsigned words_per_row = kLeoTile / 4;
-    const unsigned rows_per_chunk = kLeoThreads / words_per_row;
+    const unsigned rows_per_chunk = blockDim.x / words_per_row;
     const unsigned x_local = threadIdx.x / words_per_row, word = threadIdx.x % words_per_row;
     for (unsigned base = 0; base < n; base += rows_per_chunk) {
         const unsigned x = base + x_local;
@@ -297,7 +300,7 @@ __device__ void formal_derivative(uint8_t *w, unsigned n) {
 
 // Decode (leopard.go:582-647 / leopard8.go:536-631).
 template <class F>
-__global__ void __launch_bounds__(kLeoThreads) leo_decode_kernel(const __grid_constant__ LeoDecArgs a) {
+__global__ void __launch_bounds__(kLeoDecodeThreads) leo_decode_kernel(const __grid_constant__ LeoDecArgs a) {
     extern __shared__ __align__(16) uint8_t sm[];
     const bool gf8 = F::kSyms == 64;
     uint8_t *t8 = sm;
@@ -322,13 +325,13 @@ __global__ void __launch_bounds__(kLeoThreads) leo_decode_kernel(const __grid_co
     formal_derivative(w, n);
     fft_rows(f, w, m + (unsigned)a.k, n, a.skew);
     // reveal: out = work * (modulus - errloc)
-    for (int i = 0; i < a.k + a.p; i++) {
+    const unsigned total = (unsigned)(a.k + a.p) * F::kSyms;
+    for (unsigned it = threadIdx.x; it < total; it += blockDim.x) {
+        const int i = (int)(it / F::kSyms), s = (int)(it % F::kSyms);
         if (!bit(a.write, i)) continue;
         const unsigned row = i >= a.k ? (unsigned)(i - a.k) : (unsigned)i + m;
         const uint32_t lm = F::kMod - a.errloc[row];
-        uint8_t *dst = const_cast<uint8_t *>(a.shard[i]) + off;
-        for (int s = threadIdx.x; s < F::kSyms; s += blockDim.x)
-            F::store(dst, s, f.mul(F::load(w + (size_t)row * kLeoTile, s), lm));
+        F::store(const_cast<uint8_t *>(a.shard[i]) + off, s, f.mul(F::load(w + (size_t)row * kLeoTile, s), lm));
     }
 }
 
@@ -411,7 +414,7 @@ int leo_create(rsgpu_encoder *enc) {
     return RS_OK;
 }
 
-int leo_encode_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, size_t size) {
+int leo_encode_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, size_t size, cudaStream_t st) {
     if (size % 64) return RS_ERR_INVALID_SHARD_SIZE;
     const unsigned m = ceil_pow2((unsigned)enc->p);
     if (enc->total > kLeoMaxShards || 2 * m > kLeoMaxRows) {
@@ -433,15 +436,15 @@ int leo_encode_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, size_t size) 
     a.t8 = enc->leo->t8;
     const size_t smem = (size_t)2 * m * kLeoTile + (g16 ? 0 : kT8Bytes);
     const int grid = (int)(size / kLeoTile);
-    rsgpu_ctx *ctx = enc->ctx;
+    if (!st) st = enc->ctx->stream;
     if (g16) {
         rc = set_smem(leo_encode_kernel<F16>, smem);
         if (rc) return rc;
-        leo_encode_kernel<F16><<<grid, kLeoThreads, smem, ctx->stream>>>(a);
+        leo_encode_kernel<F16><<<grid, kLeoThreads, smem, st>>>(a);
     } else {
         rc = set_smem(leo_encode_kernel<F8>, smem);
         if (rc) return rc;
-        leo_encode_kernel<F8><<<grid, kLeoThreads, smem, ctx->stream>>>(a);
+        leo_encode_kernel<F8><<<grid, kLeoThreads, smem, st>>>(a);
     }
     RS_CUDA(cudaGetLastError());
     return RS_OK;
@@ -475,7 +478,7 @@ static int decode_checks(rsgpu_encoder *enc, const uint8_t *present, size_t size
 }
 
 int leo_reconstruct_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, const uint8_t *present,
-                            size_t size, int recover_all) {
+                            size_t size, int recover_all, cudaStream_t st) {
     bool nothing = false;
     int rc = decode_checks(enc, present, size, recover_all, &nothing);
     if (rc || nothing) return rc;
@@ -516,15 +519,15 @@ int leo_reconstruct_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, const ui
     a->t8 = enc->leo->t8;
     const size_t smem = (size_t)n * kLeoTile + (g16 ? 0 : kT8Bytes);
     const int grid = (int)(size / kLeoTile);
-    rsgpu_ctx *ctx = enc->ctx;
+    if (!st) st = enc->ctx->stream;
     if (g16) {
         rc = set_smem(leo_decode_kernel<F16>, smem);
         if (rc) return rc;
-        leo_decode_kernel<F16><<<grid, kLeoThreads, smem, ctx->stream>>>(*a);
+        leo_decode_kernel<F16><<<grid, kLeoDecodeThreads, smem, st>>>(*a);
     } else {
         rc = set_smem(leo_decode_kernel<F8>, smem);
         if (rc) return rc;
-        leo_decode_kernel<F8><<<grid, kLeoThreads, smem, ctx->stream>>>(*a);
+        leo_decode_kernel<F8><<<grid, kLeoDecodeThreads, smem, st>>>(*a);
     }
     RS_CUDA(cudaGetLastError());
     return RS_OK;

@@ -74,7 +74,12 @@ int leo_reconstruct(rsgpu_encoder *enc, uint8_t **shards, const uint8_t *present
                     int recover_all, uint8_t *written);
 // Enqueue-only variants on the context stream (no host synchronisation);
 // all shard pointers must be valid device buffers of `size` bytes.
-int leo_encode_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, size_t size);
+int leo_encode_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, size_t size, cudaStream_t st = nullptr);
 int leo_reconstruct_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, const uint8_t *present,
-                            size_t size, int recover_all);
+                            size_t size, int recover_all, cudaStream_t st = nullptr);
+// Batched execution on an explicit stream (batch.cu).
+int batch_run_on(rsgpu_batch *b, int mode, cudaStream_t st);
+int batch_stripe_count(const rsgpu_batch *b);
+// Copies the verify outcomes of a finished run (stream-ordered on st).
+int batch_read_flags(rsgpu_batch *b, int *ok, int n, cudaStream_t st);
 }  // namespace rsgpu

@@ -497,3 +497,114 @@ class Batch:
         nt, by = ctypes.c_longlong(), ctypes.c_double()
         check(L.lib().rsgpu_batch_info(self._h, ctypes.byref(ns), ctypes.byref(nj), ctypes.byref(nt), ctypes.byref(by)))
         return {"stripes": ns.value, "jobs": nj.value, "tiles": nt.value, "bytes": by.value}
+
+
+# ---- request server ------------------------------------------------------------
+class Server:
+    """Continuous-batching request server over device-resident stripes.
+
+    submit() queues a request (op, geometry, CUDA shard tensors); the server
+    thread admits requests in arrival order under an in-flight byte budget
+    and an HBM arena for reconstruct outputs left as None, and runs them as
+    micro-batches on `streams` streams.  poll() returns completions with
+    their submit-to-completion latency; outputs(ticket) gives the shard
+    device pointers after completion; release(ticket) frees arena outputs.
+    """
+    OPS = {"encode": RS_JOB_ENCODE, "reconstruct": RS_JOB_RECONSTRUCT,
+           "reconstruct_data": RS_JOB_RECONSTRUCT_DATA, "verify": RS_JOB_VERIFY}
+
+    def __init__(self, arena_bytes=1 << 30, inflight_budget=8 << 30, max_batch=256, streams=4, device=0):
+        self.ctx = Context.get(device)
+        h = ctypes.c_void_p()
+        check(L.lib().rsgpu_server_create(self.ctx.handle, int(arena_bytes), int(inflight_budget), int(max_batch),
+                                          int(streams), ctypes.byref(h)))
+        self._h = h
+        self._keep = {}
+
+    def _request(self, op, k, p, shards, present=None, leopard=0, tag=0):
+        n = k + p
+        ptrs = L.ptr_array([_ptr(s) if s is not None else None for s in shards])
+        req = L.RsRequest(self.OPS[op], k, p, int(leopard), _size(shards),
+                          ctypes.cast(ptrs, ctypes.c_void_p), None, int(tag), 0)
+        keep = [ptrs, shards]
+        if present is not None:
+            pres = L.u8_array(present)
+            req.present = ctypes.cast(pres, ctypes.c_void_p)
+            keep.append(pres)
+        assert len(shards) == n
+        return req, keep
+
+    def submit(self, op, k, p, shards, present=None, leopard=0, tag=0):
+        req, keep = self._request(op, k, p, shards, present, leopard, tag)
+        t = ctypes.c_uint64()
+        check(L.lib().rsgpu_server_submit(self._h, ctypes.byref(req), ctypes.byref(t)))
+        self._keep[t.value] = (req, keep)
+        return t.value
+
+    def replay(self, requests, arrivals_us):
+        """requests: list of dicts (op, k, p, shards, present, leopard, tag); open-loop arrivals."""
+        n = len(requests)
+        arr = (L.RsRequest * n)()
+        keeps = []
+        for i, r in enumerate(requests):
+            req, keep = self._request(r["op"], r["k"], r["p"], r["shards"], r.get("present"),
+                                      r.get("leopard", 0), r.get("tag", i))
+            arr[i] = req
+            keeps.append(keep)
+        times = (ctypes.c_double * n)(*[float(x) for x in arrivals_us])
+        tickets = (ctypes.c_uint64 * n)()
+        check(L.lib().rsgpu_server_replay(self._h, arr, times, n, tickets))
+        for i in range(n):
+            self._keep[tickets[i]] = (arr, keeps[i], i)
+        return list(tickets)
+
+    def _req_of(self, ticket):
+        v = self._keep[ticket]
+        return v[0][v[2]] if len(v) == 3 else v[0]
+
+    def outputs(self, ticket):
+        """Device pointers of the request's shards (reconstructed ones included)."""
+        req = self._req_of(ticket)
+        n = req.data_shards + req.parity_shards
+        arr = ctypes.cast(req.shards, ctypes.POINTER(ctypes.c_void_p))
+        return [arr[i] for i in range(n)]
+
+    def verify_result(self, ticket):
+        return bool(self._req_of(ticket).result)
+
+    def poll(self, max_n=4096):
+        buf = (L.RsCompletion * max_n)()
+        n = L.lib().rsgpu_server_poll(self._h, buf, max_n)
+        if n < 0:
+            check(n)
+        return [(buf[i].ticket, buf[i].tag, buf[i].status, buf[i].latency_us) for i in range(n)]
+
+    def wait_idle(self, timeout_ms=60000):
+        check(L.lib().rsgpu_server_wait_idle(self._h, int(timeout_ms)))
+
+    def release(self, ticket):
+        check(L.lib().rsgpu_server_release(self._h, int(ticket)))
+        self._keep.pop(ticket, None)
+
+    def stats(self):
+        st = L.RsServerStats()
+        check(L.lib().rsgpu_server_get_stats(self._h, ctypes.byref(st)))
+        return {f: getattr(st, f) for f, _ in L.RsServerStats._fields_}
+
+    def reset_stats(self):
+        check(L.lib().rsgpu_server_reset_stats(self._h))
+
+    def close(self):
+        if self._h:
+            L.lib().rsgpu_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def memcpy(dst_ptr, src_ptr, nbytes):
+    check(L.lib().rsgpu_memcpy(ctypes.c_void_p(dst_ptr), ctypes.c_void_p(src_ptr), int(nbytes)))
