@@ -49,6 +49,8 @@ def parse():
                     help="shard size; the headline workload is 64 MiB")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the secondary measurements (verify, reconstruct, batch, leopard)")
+    ap.add_argument("--extras", default="verify,reconstruct,batch,leopard,serving",
+                    help="comma list of secondary measurements to run")
     ap.add_argument("--batch-stripes", type=int, default=4096)
     ap.add_argument("--variant", type=int, default=-1,
                     help="force one GF(2^8) kernel variant instead of autotuning (profiling runs)")
@@ -355,6 +357,106 @@ def extra_leopard(dev):
     return out
 
 
+SERVE_GEOS = ((6, 3, 0), (10, 4, 0), (17, 3, 0), (1000, 200, 1))  # (k, p, leopard GF(2^16))
+SERVE_MAX = 4 << 20
+
+
+def serving_requests(pools, n, seed):
+    """C5 request mix: 60% encode / 40% reconstruct, geometry uniform over
+    SERVE_GEOS, shard size log-uniform 4 KiB - 4 MiB rounded to 64 B, erasure
+    count uniform in [1, p].  Requests address prefixes of the device pools."""
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for i in range(n):
+        gi = int(rng.integers(0, len(SERVE_GEOS)))
+        k, p, leo = SERVE_GEOS[gi]
+        pool = pools[gi]
+        size = max(64, int(np.exp(rng.uniform(np.log(4096), np.log(SERVE_MAX)))) // 64 * 64)
+        if rng.random() < 0.6:
+            reqs.append({"op": "encode", "k": k, "p": p, "leopard": leo, "size": size, "tag": i,
+                         "shards": pool["data"] + pool["enc_out"]})
+        else:
+            e = int(rng.integers(1, p + 1))
+            lost = set(int(x) for x in rng.choice(k + p, size=e, replace=False))
+            full = pool["data"] + pool["parity"]
+            reqs.append({"op": "reconstruct", "k": k, "p": p, "leopard": leo, "size": size, "tag": i,
+                         "shards": [None if j in lost else full[j] for j in range(k + p)],
+                         "present": [0 if j in lost else 1 for j in range(k + p)], "lost": sorted(lost), "geo": gi})
+    return reqs
+
+
+def extra_serving(dev, n_req=1200, load=0.7, seed=55):
+    """C5: the request server under (1) a burst of n_req requests (capacity)
+    and (2) Poisson arrivals offered at `load` x that capacity; p50/p99 of
+    submit-to-completion latency, data GB/s, and every reconstructed shard
+    compared with the original bytes."""
+    import torch
+    import reedsolomon_b200 as rs
+    g = torch.Generator(device=dev).manual_seed(seed)
+    pools = []
+    for k, p, leo in SERVE_GEOS:
+        data = [torch.randint(0, 256, (SERVE_MAX,), dtype=torch.uint8, device=dev, generator=g) for _ in range(k)]
+        parity = [torch.empty(SERVE_MAX, dtype=torch.uint8, device=dev) for _ in range(p)]
+        enc = rs.New(k, p, rs.WithLeopardGF16()) if leo else rs.New(k, p)
+        enc.Encode(data + parity)
+        pools.append({"data": data, "parity": parity,
+                      "enc_out": [torch.empty(SERVE_MAX, dtype=torch.uint8, device=dev) for _ in range(p)]})
+    torch.cuda.synchronize(dev)
+    srv = rs.Server(arena_bytes=24 << 30, inflight_budget=16 << 30, max_batch=64, streams=4, device=dev.index or 0)
+    out = {"geometries": ["RS(%d,%d)%s" % (k, p, " leopard16" if leo else "") for k, p, leo in SERVE_GEOS],
+           "requests": n_req, "mix": "60% encode / 40% reconstruct, 4 KiB-4 MiB log-uniform, erasures U[1,p]"}
+    ok = True
+
+    def phase(arrivals, seed_r):
+        nonlocal ok
+        reqs = serving_requests(pools, n_req, seed_r)
+        srv.reset_stats()
+        tickets = srv.replay(reqs, arrivals)
+        srv.wait_idle(600000)
+        done = srv.poll(len(reqs) + 16)
+        st = srv.stats()
+        fails = sum(1 for d in done if d[2] != 0)
+        ok &= fails == 0 and len(done) == len(reqs)
+        data_bytes = sum(r["k"] * r["size"] for r in reqs)
+        by_op = {}
+        lat = {t: l for t, _, _, l in done}
+        for r, t in zip(reqs, tickets):
+            by_op.setdefault(r["op"] + ("_leopard" if r["leopard"] else "_classic"), []).append(lat.get(t, 0.0))
+        # every reconstructed shard equals the original bytes
+        scratch = torch.empty(SERVE_MAX, dtype=torch.uint8, device=dev)
+        for r, t in zip(reqs, tickets):
+            if r["op"] == "reconstruct":
+                outs = srv.outputs(t)
+                full = pools[r["geo"]]["data"] + pools[r["geo"]]["parity"]
+                for j in r["lost"]:
+                    rs.memcpy(scratch.data_ptr(), outs[j], r["size"])
+                    ok &= bool(torch.equal(scratch[:r["size"]], full[j][:r["size"]]))
+            srv.release(t)
+        return {"req_per_s": round(len(reqs) / st["elapsed_s"], 1) if st["elapsed_s"] else None,
+                "data_GBps": round(data_bytes / st["elapsed_s"] / 1e9, 1) if st["elapsed_s"] else None,
+                "footprint_GBps": round(st["bytes"] / st["elapsed_s"] / 1e9, 1) if st["elapsed_s"] else None,
+                "latency_us_p50": round(st["p50_us"], 1), "latency_us_p99": round(st["p99_us"], 1),
+                "latency_us_max": round(st["max_us"], 1), "elapsed_s": round(st["elapsed_s"], 3),
+                "max_inflight_GB": round(st["max_inflight_bytes"] / 1e9, 2),
+                "p50_us_by_kind": {kk: round(_pct(v, 50), 1) for kk, v in sorted(by_op.items())},
+                "p99_us_by_kind": {kk: round(_pct(v, 99), 1) for kk, v in sorted(by_op.items())}}
+
+    phase([0.0] * 64, seed + 100)  # warm: encoders, tables, error locators of the warm patterns
+    burst = phase([0.0] * n_req, seed + 1)
+    out["burst"] = burst
+    rate = load * burst["req_per_s"]
+    rng = np.random.default_rng(seed + 2)
+    arrivals = np.cumsum(rng.exponential(1e6 / rate, n_req)).tolist()
+    poisson = phase(arrivals, seed + 3)
+    poisson["offered_req_per_s"] = round(rate, 1)
+    out["poisson"] = poisson
+    out["outputs_bit_exact"] = bool(ok)
+    srv.close()
+    del pools
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -430,10 +532,18 @@ def run_ours(args):
 
     extras = None
     if not args.no_extras:
-        extras = {"verify": extra_verify(enc, shards)}
-        extras.update(extra_reconstruct(enc, lib, shards, S, stream))
-        extras["batch"] = extra_batch(dev, args.batch_stripes)
-        extras["leopard"] = extra_leopard(dev)
+        want = set(args.extras.split(","))
+        extras = {}
+        if "verify" in want:
+            extras["verify"] = extra_verify(enc, shards)
+        if "reconstruct" in want:
+            extras.update(extra_reconstruct(enc, lib, shards, S, stream))
+        if "batch" in want:
+            extras["batch"] = extra_batch(dev, args.batch_stripes)
+        if "leopard" in want:
+            extras["leopard"] = extra_leopard(dev)
+        if "serving" in want:
+            extras["serving"] = extra_serving(dev)
     out = None
     if rank == 0:
         out = {

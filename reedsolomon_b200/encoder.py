@@ -521,10 +521,12 @@ class Server:
         self._h = h
         self._keep = {}
 
-    def _request(self, op, k, p, shards, present=None, leopard=0, tag=0):
+    def _request(self, op, k, p, shards, present=None, leopard=0, tag=0, size=None):
+        """`size` (bytes per shard) defaults to the length of the first shard;
+        a smaller size codes that prefix of every shard buffer."""
         n = k + p
         ptrs = L.ptr_array([_ptr(s) if s is not None else None for s in shards])
-        req = L.RsRequest(self.OPS[op], k, p, int(leopard), _size(shards),
+        req = L.RsRequest(self.OPS[op], k, p, int(leopard), int(size) if size is not None else _size(shards),
                           ctypes.cast(ptrs, ctypes.c_void_p), None, int(tag), 0)
         keep = [ptrs, shards]
         if present is not None:
@@ -534,21 +536,21 @@ class Server:
         assert len(shards) == n
         return req, keep
 
-    def submit(self, op, k, p, shards, present=None, leopard=0, tag=0):
-        req, keep = self._request(op, k, p, shards, present, leopard, tag)
+    def submit(self, op, k, p, shards, present=None, leopard=0, tag=0, size=None):
+        req, keep = self._request(op, k, p, shards, present, leopard, tag, size)
         t = ctypes.c_uint64()
         check(L.lib().rsgpu_server_submit(self._h, ctypes.byref(req), ctypes.byref(t)))
         self._keep[t.value] = (req, keep)
         return t.value
 
     def replay(self, requests, arrivals_us):
-        """requests: list of dicts (op, k, p, shards, present, leopard, tag); open-loop arrivals."""
+        """requests: list of dicts (op, k, p, shards, present, leopard, tag, size); open-loop arrivals."""
         n = len(requests)
         arr = (L.RsRequest * n)()
         keeps = []
         for i, r in enumerate(requests):
             req, keep = self._request(r["op"], r["k"], r["p"], r["shards"], r.get("present"),
-                                      r.get("leopard", 0), r.get("tag", i))
+                                      r.get("leopard", 0), r.get("tag", i), r.get("size"))
             arr[i] = req
             keeps.append(keep)
         times = (ctypes.c_double * n)(*[float(x) for x in arrivals_us])
