@@ -40,7 +40,9 @@ enum GfVariant : int {
     kVariantMulHi = 1,  // shifts as mul.hi on the FMA pipe, mask/or on the ALU pipe
     kVariantPrmt = 2,   // nibble*4 bytes, PRMT merges them into the table base
     kVariantFixed = 3,  // PRMT addressing, input loop unrolled for the exact input count
-    kNumVariants = 4,
+    kVariantFixed2 = 4, // as kVariantFixed, registers capped for 2 resident CTAs per SM
+    kVariantFixed3 = 5, // as kVariantFixed, registers capped for 3 resident CTAs per SM
+    kNumVariants = 6,
 };
 
 // Force a variant for every launch (-1 restores the tuned / default choice).

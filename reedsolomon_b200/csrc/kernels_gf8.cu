@@ -272,34 +272,44 @@ ByteKernel pick_bytes(int mode) {
 }
 
 // Specialised input counts (fully unrolled); others use gf8_matmul_vec.
-template <int N, int G>
+// MINB is the resident-CTA floor given to the register allocator: 1 lets
+// the unrolled loop keep ~160 registers (8 warps per SM), 2 caps it at 128
+// (16 warps), 3 at 80 (24 warps); none of them spills.
+template <int N, int G, int MINB>
 VecKernel pick_fixed(int mode) {
-    if (mode == kModeWrite) return gf8_matmul_fixed<N, G, kModeWrite, kVariantPrmt, FIXED_MINB>;
-    if (mode == kModeXor) return gf8_matmul_fixed<N, G, kModeXor, kVariantPrmt, FIXED_MINB>;
-    return gf8_matmul_fixed<N, G, kModeVerify, kVariantPrmt, FIXED_MINB>;
+    if (mode == kModeWrite) return gf8_matmul_fixed<N, G, kModeWrite, kVariantPrmt, MINB>;
+    if (mode == kModeXor) return gf8_matmul_fixed<N, G, kModeXor, kVariantPrmt, MINB>;
+    return gf8_matmul_fixed<N, G, kModeVerify, kVariantPrmt, MINB>;
 }
 
-template <int G>
+template <int G, int MINB>
 VecKernel fixed_for_g(int n_in, int mode) {
     switch (n_in) {
-    case 4: return pick_fixed<4, G>(mode);
-    case 5: return pick_fixed<5, G>(mode);
-    case 6: return pick_fixed<6, G>(mode);
-    case 8: return pick_fixed<8, G>(mode);
-    case 10: return pick_fixed<10, G>(mode);
-    case 12: return pick_fixed<12, G>(mode);
-    case 16: return pick_fixed<16, G>(mode);
-    case 17: return pick_fixed<17, G>(mode);
-    case 20: return pick_fixed<20, G>(mode);
+    case 4: return pick_fixed<4, G, MINB>(mode);
+    case 5: return pick_fixed<5, G, MINB>(mode);
+    case 6: return pick_fixed<6, G, MINB>(mode);
+    case 8: return pick_fixed<8, G, MINB>(mode);
+    case 10: return pick_fixed<10, G, MINB>(mode);
+    case 12: return pick_fixed<12, G, MINB>(mode);
+    case 16: return pick_fixed<16, G, MINB>(mode);
+    case 17: return pick_fixed<17, G, MINB>(mode);
+    case 20: return pick_fixed<20, G, MINB>(mode);
     }
     return nullptr;
 }
 
-// nullptr when no specialisation exists for (n_in, G).
-VecKernel fixed_kernel(int n_in, int G, int mode) {
-    if (G == 1) return fixed_for_g<1>(n_in, mode);
-    if (G == 2) return fixed_for_g<2>(n_in, mode);
+template <int MINB>
+VecKernel fixed_for_minb(int n_in, int G, int mode) {
+    if (G == 1) return fixed_for_g<1, MINB>(n_in, mode);
+    if (G == 2) return fixed_for_g<2, MINB>(n_in, mode);
     return nullptr;
+}
+
+// nullptr when no specialisation exists for (n_in, G).
+VecKernel fixed_kernel(int n_in, int G, int mode, int variant) {
+    if (variant == kVariantFixed2) return fixed_for_minb<2>(n_in, G, mode);
+    if (variant == kVariantFixed3) return fixed_for_minb<3>(n_in, G, mode);
+    return fixed_for_minb<FIXED_MINB>(n_in, G, mode);
 }
 
 VecKernel vec_kernel(int G, int mode, int v) {
@@ -400,8 +410,9 @@ cudaError_t launch_gf8_tile(cudaStream_t st, const DeviceInfo &dev, const GfMatA
         const long long nvec = a.nbytes >> 4;
         if (nvec > 0) {
             VecKernel kern = nullptr;
-            if (variant == kVariantFixed) kern = fixed_kernel(a.n_in, G, mode);
-            if (!kern) kern = vec_kernel(G, mode, variant == kVariantFixed ? kVariantPrmt : variant);
+            const bool fixed = variant == kVariantFixed || variant == kVariantFixed2 || variant == kVariantFixed3;
+            if (fixed) kern = fixed_kernel(a.n_in, G, mode, variant);
+            if (!kern) kern = vec_kernel(G, mode, fixed ? kVariantPrmt : variant);
             const long long want = (nvec + kThreads - 1) / kThreads;
             const long long cap = (long long)dev.sm_count * blocks_per_sm(kern, smem);
             const int grid = (int)std::max(1LL, std::min(want, cap));

@@ -12,10 +12,13 @@
 // is touched once per shard: algorithmic bytes = (k + p) * size for encode,
 // (present + written) * size for decode.
 //
-// Multiplication by a constant log value lm uses nibble product tables
-// (4 x 16 u16 per lm for GF(2^16), 8 MB in global memory, L1/L2 resident;
-// 2 x 16 bytes per lm for GF(2^8), 8 KB in shared memory).  Butterfly groups
-// are warp-uniform, so a warp's table reads hit one 32-byte sector.
+// Multiplication by a constant log value lm uses split product tables
+// (GF(2^16): 64 + 64 + 16 u16 per lm for symbol bits 0-5, 6-11, 12-15, 32 MB
+// in global memory, L1/L2 resident, three lookups per symbol; GF(2^8):
+// 2 x 16 bytes per lm, 8 KB in shared memory).  Each thread handles four
+// symbols of a row per butterfly, and a warp's lanes share their
+// multipliers once the butterfly distance reaches 4, so a lookup reads one
+// 128-byte line per warp.
 #include <algorithm>
 #include <cstring>
 
@@ -34,7 +37,7 @@ constexpr int kLeoMaxRows = 2048;     // rows held in shared memory (2048 * 64 B
 struct LeoState {
     int device = -1;
     uint16_t *skew16 = nullptr;  // fftSkew, 65535 entries
-    uint16_t *t16 = nullptr;     // [65536][4][16] nibble products
+    uint16_t *t16 = nullptr;     // [65536][kT16Stride] split product tables (see F16)
     uint16_t *skew8 = nullptr;   // fftSkew8, 255 entries (widened)
     uint8_t *t8 = nullptr;       // [256][2][16] nibble products
     ErrLocCache errlocs;
@@ -49,6 +52,8 @@ struct LeoState {
 };
 
 namespace {
+
+constexpr int kT16Stride = 256;  // u16 entries per log value (512 bytes, 4 L1 lines)
 
 struct LeoEncArgs {
     const uint8_t *shard[kLeoMaxShards];  // k data then p parity pointers
@@ -74,47 +79,97 @@ struct LeoDecArgs {
 __device__ __forceinline__ bool bit(const uint32_t *v, int i) { return (v[i >> 5] >> (i & 31)) & 1u; }
 
 // ---- field policies -----------------------------------------------------
+// A thread works on a "quad": 4 consecutive symbols of one 64-byte row tile.
+// GF(2^16) rows hold 32 symbols as 32 low bytes | 32 high bytes
+// (leopard.go:907-925), so a quad is the u32 word of low bytes at 4q and
+// the word of high bytes at 32 + 4q; GF(2^8) rows hold 64 byte symbols, a
+// quad is one u32 word.  Consecutive threads take consecutive quads of a
+// row, so a warp covers 4 (GF(2^16)) or 2 (GF(2^8)) butterfly positions,
+// which share their multipliers whenever the butterfly distance is >= 4.
 struct F16 {
     static constexpr unsigned kMod = 65535;
-    static constexpr int kSyms = 32;  // symbols per 64-byte row tile
-    static __device__ __forceinline__ uint32_t load(const uint8_t *row, int s) {
-        return (uint32_t)row[s] | ((uint32_t)row[32 + s] << 8);
+    static constexpr int kQuads = 8;
+    static constexpr int kQuadShift = 3;
+    using Q = uint2;
+    static __device__ __forceinline__ Q ld(const uint8_t *row, int q) {
+        return make_uint2(reinterpret_cast<const uint32_t *>(row)[q], reinterpret_cast<const uint32_t *>(row + 32)[q]);
     }
-    static __device__ __forceinline__ void store(uint8_t *row, int s, uint32_t v) {
-        row[s] = (uint8_t)v;
-        row[32 + s] = (uint8_t)(v >> 8);
+    static __device__ __forceinline__ void st(uint8_t *row, int q, Q v) {
+        reinterpret_cast<uint32_t *>(row)[q] = v.x;
+        reinterpret_cast<uint32_t *>(row + 32)[q] = v.y;
     }
+    static __device__ __forceinline__ Q ldg(const uint8_t *row, int q) {
+        return make_uint2(__ldcs(reinterpret_cast<const uint32_t *>(row) + q),
+                          __ldcs(reinterpret_cast<const uint32_t *>(row + 32) + q));
+    }
+    static __device__ __forceinline__ void stg(uint8_t *row, int q, Q v) {
+        __stcs(reinterpret_cast<uint32_t *>(row) + q, v.x);
+        __stcs(reinterpret_cast<uint32_t *>(row + 32) + q, v.y);
+    }
+    static __device__ __forceinline__ Q zero() { return make_uint2(0, 0); }
+    static __device__ __forceinline__ void xor_into(Q &a, Q b) {
+        a.x ^= b.x;
+        a.y ^= b.y;
+    }
+    // Products by a log value lm split by symbol bits: T[0..64) covers bits
+    // 0-5, T[64..128) bits 6-11, T[128..144) bits 12-15.  Each part fits one
+    // 128-byte line, so a warp whose lanes share lm reads one line per lookup.
     const uint16_t *t;
-    __device__ __forceinline__ uint32_t mul(uint32_t x, uint32_t lm) const {
-        const uint16_t *T = t + (size_t)lm * 64;
-        return (uint32_t)__ldg(T + (x & 15)) ^ __ldg(T + 16 + ((x >> 4) & 15)) ^
-               __ldg(T + 32 + ((x >> 8) & 15)) ^ __ldg(T + 48 + (x >> 12));
+    static __device__ __forceinline__ uint32_t mul1(uint32_t x, const uint16_t *T) {
+        return (uint32_t)__ldg(T + (x & 63)) ^ (uint32_t)__ldg(T + 64 + ((x >> 6) & 63)) ^
+               (uint32_t)__ldg(T + 128 + ((x >> 12) & 15));
+    }
+    __device__ __forceinline__ Q mul(Q v, uint32_t lm) const {
+        const uint16_t *T = t + (size_t)lm * kT16Stride;
+        // symbol i = low byte i | high byte i << 8 (bits above 15 are ignored)
+        const uint32_t r0 = mul1(__byte_perm(v.x, v.y, 0x0040), T);
+        const uint32_t r1 = mul1(__byte_perm(v.x, v.y, 0x0051), T);
+        const uint32_t r2 = mul1(__byte_perm(v.x, v.y, 0x0062), T);
+        const uint32_t r3 = mul1(__byte_perm(v.x, v.y, 0x0073), T);
+        const uint32_t r01 = __byte_perm(r0, r1, 0x5410), r23 = __byte_perm(r2, r3, 0x5410);
+        return make_uint2(__byte_perm(r01, r23, 0x6420), __byte_perm(r01, r23, 0x7531));
     }
 };
 
 struct F8 {
     static constexpr unsigned kMod = 255;
-    static constexpr int kSyms = 64;
-    static __device__ __forceinline__ uint32_t load(const uint8_t *row, int s) { return row[s]; }
-    static __device__ __forceinline__ void store(uint8_t *row, int s, uint32_t v) { row[s] = (uint8_t)v; }
-    const uint8_t *t;  // shared copy of the 8 KB table
-    __device__ __forceinline__ uint32_t mul(uint32_t x, uint32_t lm) const {
+    static constexpr int kQuads = 16;
+    static constexpr int kQuadShift = 4;
+    using Q = uint32_t;
+    static __device__ __forceinline__ Q ld(const uint8_t *row, int q) { return reinterpret_cast<const uint32_t *>(row)[q]; }
+    static __device__ __forceinline__ void st(uint8_t *row, int q, Q v) { reinterpret_cast<uint32_t *>(row)[q] = v; }
+    static __device__ __forceinline__ Q ldg(const uint8_t *row, int q) {
+        return __ldcs(reinterpret_cast<const uint32_t *>(row) + q);
+    }
+    static __device__ __forceinline__ void stg(uint8_t *row, int q, Q v) {
+        __stcs(reinterpret_cast<uint32_t *>(row) + q, v);
+    }
+    static __device__ __forceinline__ Q zero() { return 0; }
+    static __device__ __forceinline__ void xor_into(Q &a, Q b) { a ^= b; }
+    const uint8_t *t;  // shared copy of the 8 KB table: [lm][lo nibble 16 | hi nibble 16]
+    __device__ __forceinline__ Q mul(Q v, uint32_t lm) const {
         const uint8_t *T = t + lm * 32;
-        return (uint32_t)T[x & 15] ^ T[16 + (x >> 4)];
+        uint32_t r = 0;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const uint32_t b = (v >> (8 * i)) & 255u;
+            r |= (uint32_t)(T[b & 15] ^ T[16 + (b >> 4)]) << (8 * i);
+        }
+        return r;
     }
 };
 
 // Butterflies (galois_noasm.go:94-112; a log multiplier equal to the modulus
 // stands for multiplication by zero and reduces the butterfly to an XOR).
 template <class F>
-__device__ __forceinline__ void fft2(const F &f, uint32_t &x, uint32_t &y, uint32_t lm) {
-    if (lm != F::kMod) x ^= f.mul(y, lm);
-    y ^= x;
+__device__ __forceinline__ void fft2(const F &f, typename F::Q &x, typename F::Q &y, uint32_t lm) {
+    if (lm != F::kMod) F::xor_into(x, f.mul(y, lm));
+    F::xor_into(y, x);
 }
 template <class F>
-__device__ __forceinline__ void ifft2(const F &f, uint32_t &x, uint32_t &y, uint32_t lm) {
-    y ^= x;
-    if (lm != F::kMod) x ^= f.mul(y, lm);
+__device__ __forceinline__ void ifft2(const F &f, typename F::Q &x, typename F::Q &y, uint32_t lm) {
+    F::xor_into(y, x);
+    if (lm != F::kMod) F::xor_into(x, f.mul(y, lm));
 }
 
 // IFFT with decimation in time (ifftDITEncoder leopard.go:764-873 with
@@ -123,12 +178,13 @@ __device__ __forceinline__ void ifft2(const F &f, uint32_t &x, uint32_t &y, uint
 template <class F>
 __device__ void ifft_rows(const F &f, uint8_t *w, unsigned mtrunc, unsigned m, const uint16_t *skew,
                           int skew_off) {
+    using Q = typename F::Q;
     unsigned dist = 1, dist4 = 4, ld = 0;  // dist == 1 << ld
     for (; dist4 <= m; dist = dist4, dist4 <<= 2, ld += 2) {
         const unsigned groups = (mtrunc + dist4 - 1) >> (ld + 2);
-        const unsigned items = (groups << ld) * F::kSyms;
+        const unsigned items = (groups << ld) << F::kQuadShift;
         for (unsigned it = threadIdx.x; it < items; it += blockDim.x) {
-            const unsigned q = it / F::kSyms, s = it % F::kSyms;
+            const unsigned q = it >> F::kQuadShift, c = it & (F::kQuads - 1);
             const unsigned r = (q >> ld) << (ld + 2), i = r + (q & (dist - 1)), iend = r + dist;
             const uint32_t m01 = skew[skew_off + (int)iend];
             const uint32_t m02 = skew[skew_off + (int)(iend + dist)];
@@ -136,28 +192,28 @@ __device__ void ifft_rows(const F &f, uint8_t *w, unsigned mtrunc, unsigned m, c
             uint8_t *p0 = w + (size_t)i * kLeoTile;
             uint8_t *p1 = p0 + (size_t)dist * kLeoTile, *p2 = p1 + (size_t)dist * kLeoTile,
                     *p3 = p2 + (size_t)dist * kLeoTile;
-            uint32_t x0 = F::load(p0, s), x1 = F::load(p1, s), x2 = F::load(p2, s), x3 = F::load(p3, s);
+            Q x0 = F::ld(p0, c), x1 = F::ld(p1, c), x2 = F::ld(p2, c), x3 = F::ld(p3, c);
             ifft2(f, x0, x1, m01);
             ifft2(f, x2, x3, m23);
             ifft2(f, x0, x2, m02);
             ifft2(f, x1, x3, m02);
-            F::store(p0, s, x0);
-            F::store(p1, s, x1);
-            F::store(p2, s, x2);
-            F::store(p3, s, x3);
+            F::st(p0, c, x0);
+            F::st(p1, c, x1);
+            F::st(p2, c, x2);
+            F::st(p3, c, x3);
         }
         __syncthreads();
     }
     if (dist < m) {  // one radix-2 layer left (dist == m / 2)
         const uint32_t lm = skew[skew_off + (int)dist];
-        const unsigned items = dist * F::kSyms;
+        const unsigned items = dist << F::kQuadShift;
         for (unsigned it = threadIdx.x; it < items; it += blockDim.x) {
-            const unsigned i = it / F::kSyms, s = it % F::kSyms;
+            const unsigned i = it >> F::kQuadShift, c = it & (F::kQuads - 1);
             uint8_t *p0 = w + (size_t)i * kLeoTile, *p1 = p0 + (size_t)dist * kLeoTile;
-            uint32_t x = F::load(p0, s), y = F::load(p1, s);
+            Q x = F::ld(p0, c), y = F::ld(p1, c);
             ifft2(f, x, y, lm);
-            F::store(p0, s, x);
-            F::store(p1, s, y);
+            F::st(p0, c, x);
+            F::st(p1, c, y);
         }
         __syncthreads();
     }
@@ -167,41 +223,42 @@ __device__ void ifft_rows(const F &f, uint8_t *w, unsigned mtrunc, unsigned m, c
 // skew[iend-1], [iend+dist-1], [iend+2*dist-1]; groups start below mtrunc.
 template <class F>
 __device__ void fft_rows(const F &f, uint8_t *w, unsigned mtrunc, unsigned m, const uint16_t *skew) {
+    using Q = typename F::Q;
     unsigned dist4 = m, dist = m >> 2;
     unsigned ld = 0;  // dist == 1 << ld
     while ((2u << ld) <= dist) ld++;
     for (; dist != 0; dist4 = dist, dist >>= 2, ld -= 2) {
         const unsigned groups = (mtrunc + dist4 - 1) >> (ld + 2);
-        const unsigned items = (groups << ld) * F::kSyms;
+        const unsigned items = (groups << ld) << F::kQuadShift;
         for (unsigned it = threadIdx.x; it < items; it += blockDim.x) {
-            const unsigned q = it / F::kSyms, s = it % F::kSyms;
+            const unsigned q = it >> F::kQuadShift, c = it & (F::kQuads - 1);
             const unsigned r = (q >> ld) << (ld + 2), i = r + (q & (dist - 1)), iend = r + dist;
             const uint32_t m01 = skew[iend - 1], m02 = skew[iend + dist - 1], m23 = skew[iend + 2 * dist - 1];
             uint8_t *p0 = w + (size_t)i * kLeoTile;
             uint8_t *p1 = p0 + (size_t)dist * kLeoTile, *p2 = p1 + (size_t)dist * kLeoTile,
                     *p3 = p2 + (size_t)dist * kLeoTile;
-            uint32_t x0 = F::load(p0, s), x1 = F::load(p1, s), x2 = F::load(p2, s), x3 = F::load(p3, s);
+            Q x0 = F::ld(p0, c), x1 = F::ld(p1, c), x2 = F::ld(p2, c), x3 = F::ld(p3, c);
             fft2(f, x0, x2, m02);
             fft2(f, x1, x3, m02);
             fft2(f, x0, x1, m01);
             fft2(f, x2, x3, m23);
-            F::store(p0, s, x0);
-            F::store(p1, s, x1);
-            F::store(p2, s, x2);
-            F::store(p3, s, x3);
+            F::st(p0, c, x0);
+            F::st(p1, c, x1);
+            F::st(p2, c, x2);
+            F::st(p3, c, x3);
         }
         __syncthreads();
     }
     if (dist4 == 2) {
-        const unsigned items = ((mtrunc + 1) / 2) * F::kSyms;
+        const unsigned items = ((mtrunc + 1) / 2) << F::kQuadShift;
         for (unsigned it = threadIdx.x; it < items; it += blockDim.x) {
-            const unsigned r = 2 * (it / F::kSyms), s = it % F::kSyms;
+            const unsigned r = 2 * (it >> F::kQuadShift), c = it & (F::kQuads - 1);
             const uint32_t lm = skew[r];
             uint8_t *p0 = w + (size_t)r * kLeoTile, *p1 = p0 + kLeoTile;
-            uint32_t x = F::load(p0, s), y = F::load(p1, s);
+            Q x = F::ld(p0, c), y = F::ld(p1, c);
             fft2(f, x, y, lm);
-            F::store(p0, s, x);
-            F::store(p1, s, y);
+            F::st(p0, c, x);
+            F::st(p1, c, y);
         }
         __syncthreads();
     }
@@ -238,7 +295,7 @@ constexpr int kT8Bytes = 256 * 32;
 template <class F>
 __global__ void __launch_bounds__(kLeoThreads) leo_encode_kernel(const __grid_constant__ LeoEncArgs a) {
     extern __shared__ __align__(16) uint8_t sm[];
-    const bool gf8 = F::kSyms == 64;
+    const bool gf8 = F::kQuads == 16;
     uint8_t *t8 = sm;
     uint8_t *acc = sm + (gf8 ? kT8Bytes : 0);
     const unsigned m = (unsigned)a.m;
@@ -302,7 +359,7 @@ __device__ void formal_derivative(uint8_t *w, unsigned n) {
 template <class F>
 __global__ void __launch_bounds__(kLeoDecodeThreads) leo_decode_kernel(const __grid_constant__ LeoDecArgs a) {
     extern __shared__ __align__(16) uint8_t sm[];
-    const bool gf8 = F::kSyms == 64;
+    const bool gf8 = F::kQuads == 16;
     uint8_t *t8 = sm;
     uint8_t *w = sm + (gf8 ? kT8Bytes : 0);
     if (gf8) load_tables8<F>(t8, a.t8);
@@ -311,35 +368,41 @@ __global__ void __launch_bounds__(kLeoDecodeThreads) leo_decode_kernel(const __g
     const long long off = (long long)blockIdx.x * kLeoTile;
     const unsigned n = (unsigned)a.n, m = (unsigned)a.m;
     // work <- received symbols scaled by their error locators; zeros elsewhere
-    for (unsigned it = threadIdx.x; it < n * F::kSyms; it += blockDim.x) {
-        const unsigned r = it / F::kSyms, s = it % F::kSyms;
+    using Q = typename F::Q;
+    for (unsigned it = threadIdx.x; it < (n << F::kQuadShift); it += blockDim.x) {
+        const unsigned r = it >> F::kQuadShift, c = it & (F::kQuads - 1);
         int src = -1;
         if (r < (unsigned)a.p) src = a.k + (int)r;
         else if (r >= m && r < m + (unsigned)a.k) src = (int)(r - m);
-        uint32_t v = 0;
-        if (src >= 0 && bit(a.present, src)) v = f.mul(F::load(a.shard[src] + off, s), a.errloc[r]);
-        F::store(w + (size_t)r * kLeoTile, s, v);
+        Q v = F::zero();
+        if (src >= 0 && bit(a.present, src)) v = f.mul(F::ldg(a.shard[src] + off, c), a.errloc[r]);
+        F::st(w + (size_t)r * kLeoTile, c, v);
     }
     __syncthreads();
     ifft_rows(f, w, (unsigned)a.input_count, n, a.skew, -1);
     formal_derivative(w, n);
     fft_rows(f, w, m + (unsigned)a.k, n, a.skew);
     // reveal: out = work * (modulus - errloc)
-    const unsigned total = (unsigned)(a.k + a.p) * F::kSyms;
+    const unsigned total = (unsigned)(a.k + a.p) << F::kQuadShift;
     for (unsigned it = threadIdx.x; it < total; it += blockDim.x) {
-        const int i = (int)(it / F::kSyms), s = (int)(it % F::kSyms);
+        const int i = (int)(it >> F::kQuadShift), c = (int)(it & (F::kQuads - 1));
         if (!bit(a.write, i)) continue;
         const unsigned row = i >= a.k ? (unsigned)(i - a.k) : (unsigned)i + m;
         const uint32_t lm = F::kMod - a.errloc[row];
-        F::store(const_cast<uint8_t *>(a.shard[i]) + off, s, f.mul(F::load(w + (size_t)row * kLeoTile, s), lm));
+        F::stg(const_cast<uint8_t *>(a.shard[i]) + off, c, f.mul(F::ld(w + (size_t)row * kLeoTile, c), lm));
     }
 }
 
-// Builds [65536][4][16] nibble products: mulLog(e << 4q, lm).
+// Builds the [65536][kT16Stride] split product tables of F16:
+// mulLog(j, lm), mulLog(j << 6, lm), mulLog(j << 12, lm) (leopard.go:1008-1014).
 __global__ void build_t16(uint16_t *t, const uint16_t *log, const uint16_t *exp) {
-    for (unsigned idx = blockIdx.x * blockDim.x + threadIdx.x; idx < 65536u * 64u; idx += gridDim.x * blockDim.x) {
-        const unsigned lm = idx >> 6, q = (idx >> 4) & 3, e = idx & 15;
-        const unsigned x = e << (4 * q);
+    for (unsigned idx = blockIdx.x * blockDim.x + threadIdx.x; idx < 65536u * kT16Stride;
+         idx += gridDim.x * blockDim.x) {
+        const unsigned lm = idx / kT16Stride, j = idx % kT16Stride;
+        unsigned x = 0;
+        if (j < 64) x = j;
+        else if (j < 128) x = (j - 64) << 6;
+        else if (j < 144) x = (j - 128) << 12;
         uint16_t v = 0;
         if (x) {
             unsigned s = (unsigned)log[x] + lm;
@@ -362,7 +425,7 @@ int ensure_tables(rsgpu_encoder *enc) {
     const Leo16 &f16 = Leo16::get();
     const Leo8 &f8 = Leo8::get();
     RS_CUDA(cudaMalloc(&st->skew16, 65535 * 2));
-    RS_CUDA(cudaMalloc(&st->t16, 65536ull * 64 * 2));
+    RS_CUDA(cudaMalloc(&st->t16, 65536ull * kT16Stride * 2));
     RS_CUDA(cudaMalloc(&st->skew8, 255 * 2));
     RS_CUDA(cudaMalloc(&st->t8, kT8Bytes));
     RS_CUDA(cudaMemcpy(st->skew16, f16.skew.data(), 65535 * 2, cudaMemcpyHostToDevice));
@@ -398,6 +461,14 @@ bool encode_fits(const rsgpu_encoder *enc) {
     return max_index < (is16(enc) ? 65535u : 255u);
 }
 
+// The kernels move shard data in 16-byte (encode) and 4-byte (decode)
+// vectors, so every buffer they touch must be 16-byte aligned.
+bool shards_aligned(const uint8_t *const *shards, int n) {
+    for (int i = 0; i < n; i++)
+        if (shards[i] && (reinterpret_cast<uintptr_t>(shards[i]) & 15u)) return false;
+    return true;
+}
+
 template <class K>
 int set_smem(K kern, size_t bytes) {
     RS_CUDA(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
@@ -419,6 +490,10 @@ int leo_encode_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, size_t size, 
     const unsigned m = ceil_pow2((unsigned)enc->p);
     if (enc->total > kLeoMaxShards || 2 * m > kLeoMaxRows) {
         set_error("leopard encode: geometry exceeds the shared-memory transform (k+p <= 2048, 2*ceilPow2(p) <= 2048)");
+        return RS_ERR_NOT_SUPPORTED;
+    }
+    if (!shards_aligned(shards, enc->total)) {
+        set_error("leopard encode: shard buffers must be 16-byte aligned");
         return RS_ERR_NOT_SUPPORTED;
     }
     int rc = ensure_tables(enc);
@@ -488,6 +563,10 @@ int leo_reconstruct_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, const ui
         set_error("leopard decode: geometry exceeds the shared-memory transform (ceilPow2(ceilPow2(p)+k) <= 2048)");
         return RS_ERR_NOT_SUPPORTED;
     }
+    if (!shards_aligned(shards, enc->total)) {
+        set_error("leopard reconstruct: shard buffers must be 16-byte aligned");
+        return RS_ERR_NOT_SUPPORTED;
+    }
     rc = ensure_tables(enc);
     if (rc) return rc;
     const bool g16 = is16(enc);
@@ -540,6 +619,10 @@ int leo_reconstruct(rsgpu_encoder *enc, uint8_t **shards, const uint8_t *present
     int rc = decode_checks(enc, present, size, recover_all, &nothing);
     if (rc || nothing) return rc;
     const int end = recover_all ? enc->total : enc->k;
+    if (!shards_aligned(shards, enc->total)) {  // before allocating anything
+        set_error("leopard reconstruct: shard buffers must be 16-byte aligned");
+        return RS_ERR_NOT_SUPPORTED;
+    }
     for (int i = 0; i < enc->total; i++) {
         if (present[i]) {
             if (!shards[i]) return RS_ERR_SHARD_SIZE;

@@ -143,3 +143,17 @@ def test_leopard_errors_and_host_path():
     cp = [None, None, None, None, None] + [dev(a) for a in ref[5:]]
     with pytest.raises(rs.ErrTooFewShards):
         rs.New(10, 4, rs.WithLeopardGF16()).Reconstruct(cp)
+
+
+@pytest.mark.parametrize("gf", [16, 8])
+def test_leopard_rejects_misaligned_shards(gf):
+    """Shard buffers off a 16-byte boundary are refused on the host before any launch."""
+    k, p, size = 5, 3, 128
+    base = torch.zeros((k + p) * (size + 16) + 16, dtype=torch.uint8, device="cuda")
+    sh = [base[1 + i * (size + 16):1 + i * (size + 16) + size] for i in range(k + p)]
+    enc = new(gf, k, p)
+    with pytest.raises(rs.ErrNotSupported):
+        enc.Encode(sh)
+    sh[0] = None
+    with pytest.raises(rs.ErrNotSupported):
+        enc.Reconstruct(sh)
