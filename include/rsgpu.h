@@ -224,9 +224,12 @@ int rsgpu_batch_set_tile(rsgpu_batch *batch, int tile_bytes);
  * requests; a server thread admits them in arrival order while the bytes of
  * work in flight stay under `inflight_budget` and reconstruct outputs without
  * a caller buffer fit in an HBM arena of `arena_bytes`, and launches each
- * admitted group as one micro-batch on one of `streams` streams, so requests
- * arriving while others run are admitted as soon as a stream frees up and
- * their work overlaps on the device. */
+ * admitted group as one micro-batch on a free stream, so requests arriving
+ * while others run are admitted as soon as a stream frees up and their work
+ * overlaps on the device.  Classic and Leopard requests queue in separate
+ * lanes of `streams` streams each (classic on high-priority streams); the
+ * Leopard lane holds at most 3/4 of the budget, so classic requests are
+ * never queued behind Leopard ones. */
 typedef struct rsgpu_request {
     int op;                     /* RS_JOB_* (verify: classic stripes only) */
     int data_shards, parity_shards;

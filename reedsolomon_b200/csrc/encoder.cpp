@@ -18,6 +18,7 @@ static thread_local std::string g_last_error;
 void set_error(const std::string &msg) { g_last_error = msg; }
 
 int cuda_status(cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return RS_OK;
     char buf[512];
     snprintf(buf, sizeof buf, "%s: %s (%d)", what, cudaGetErrorString(e), (int)e);
     set_error(buf);

@@ -374,7 +374,10 @@ int choose_variant(int n_in, int n_out, int mode, size_t nbytes) {
     if (g_forced >= 0) return g_forced;
     auto it = g_tuned.find(std::make_tuple(n_in, (n_out + 3) / 4, mode, size_bucket(nbytes)));
     if (it != g_tuned.end()) return it->second;
-    return kVariantFixed;  // fastest in every measured geometry; falls back to kVariantPrmt
+    // Untuned default: the unrolled kernel with the largest register cap that
+    // does not spill (3 CTAs per SM for up to 4 outputs, 2 for 5-8 outputs);
+    // input counts without a specialisation fall back to kVariantPrmt.
+    return n_out <= 4 ? kVariantFixed3 : kVariantFixed2;
 }
 
 void record_variant(int n_in, int n_out, int mode, size_t nbytes, int v) {

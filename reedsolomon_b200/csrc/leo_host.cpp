@@ -102,55 +102,4 @@ const LeoField<BITS> &LeoField<BITS>::get() {
 template struct LeoField<16>;
 template struct LeoField<8>;
 
-// leopard.go:468-510: ones at erased positions (parity first, data at offset
-// m, the padding rows p..m-1 always), FWHT, times FWHT(log), FWHT again.
-template <int BITS>
-static std::vector<uint16_t> errlocs_impl(int k, int p, const uint8_t *present) {
-    const LeoField<BITS> &f = LeoField<BITS>::get();
-    const unsigned m = ceil_pow2((unsigned)p);
-    std::vector<uint16_t> el(f.kOrder, 0);
-    for (int i = 0; i < p; i++)
-        if (!present[k + i]) el[i] = 1;
-    for (unsigned i = (unsigned)p; i < m; i++) el[i] = 1;
-    for (int i = 0; i < k; i++)
-        if (!present[i]) el[m + i] = 1;
-    fwht<BITS>(el.data(), m + (unsigned)k);
-    for (unsigned i = 0; i < f.kOrder; i++) el[i] = (uint16_t)(((uint32_t)el[i] * f.walsh[i]) % f.kMod);
-    fwht<BITS>(el.data(), f.kOrder);
-    return el;
-}
-
-std::vector<uint16_t> leo_errlocs(int bits, int k, int p, const uint8_t *present) {
-    return bits == 16 ? errlocs_impl<16>(k, p, present) : errlocs_impl<8>(k, p, present);
-}
-
-std::shared_ptr<const std::vector<uint16_t>> ErrLocCache::get(int bits, int k, int p,
-                                                             const uint8_t *present) {
-    std::string key;
-    key.reserve((size_t)(k + p) + 16);
-    key.append(reinterpret_cast<const char *>(&bits), sizeof bits);
-    key.append(reinterpret_cast<const char *>(&k), sizeof k);
-    key.append(reinterpret_cast<const char *>(&p), sizeof p);
-    for (int i = 0; i < k + p; i++) key.push_back(present[i] ? 1 : 0);
-    {
-        std::lock_guard<std::mutex> lk(mu_);
-        auto it = map_.find(key);
-        if (it != map_.end()) {
-            lru_.splice(lru_.begin(), lru_, it->second.second);
-            return it->second.first;
-        }
-    }
-    auto val = std::make_shared<const std::vector<uint16_t>>(leo_errlocs(bits, k, p, present));
-    std::lock_guard<std::mutex> lk(mu_);
-    if (map_.find(key) == map_.end()) {
-        if (map_.size() >= cap_) {
-            map_.erase(lru_.back());
-            lru_.pop_back();
-        }
-        lru_.push_front(key);
-        map_.emplace(key, std::make_pair(val, lru_.begin()));
-    }
-    return val;
-}
-
 }  // namespace rsgpu

@@ -1,17 +1,11 @@
 // leo_host.h -- host-side Leopard field tables and error locators.
 //
 // Restates the table construction of leopard.go:1104-1274 (GF(2^16)) and
-// leopard8.go:1029-1137 (GF(2^8)) and the error-locator evaluation of
-// leopard.go:468-510 / leopard8.go:434-513, which stays on the host (FWHT over
-// the field order per erasure pattern, cached per pattern).
+// leopard8.go:1029-1137 (GF(2^8)).  The per-pattern error locators are
+// computed on the device (leo_errloc_kernel in leopard.cu).
 #pragma once
 
 #include <cstdint>
-#include <list>
-#include <map>
-#include <memory>
-#include <mutex>
-#include <string>
 #include <vector>
 
 namespace rsgpu {
@@ -32,23 +26,6 @@ struct LeoField {
 
 using Leo16 = LeoField<16>;
 using Leo8 = LeoField<8>;
-
-// Error locators for an erasure pattern (present[k+p]); returns kOrder values.
-// Cached per pattern (bounded LRU) like leopard8.go's inversion map.
-class ErrLocCache {
-  public:
-    explicit ErrLocCache(size_t capacity = 256) : cap_(capacity) {}
-    std::shared_ptr<const std::vector<uint16_t>> get(int bits, int k, int p, const uint8_t *present);
-
-  private:
-    using Entry = std::shared_ptr<const std::vector<uint16_t>>;
-    size_t cap_;
-    std::mutex mu_;
-    std::list<std::string> lru_;
-    std::map<std::string, std::pair<Entry, std::list<std::string>::iterator>> map_;
-};
-
-std::vector<uint16_t> leo_errlocs(int bits, int k, int p, const uint8_t *present);
 
 inline unsigned ceil_pow2(unsigned n) {
     unsigned r = 1;

@@ -40,13 +40,16 @@ struct LeoState {
     uint16_t *t16 = nullptr;     // [65536][kT16Stride] split product tables (see F16)
     uint16_t *skew8 = nullptr;   // fftSkew8, 255 entries (widened)
     uint8_t *t8 = nullptr;       // [256][2][16] nibble products
-    ErrLocCache errlocs;
+    uint16_t *fold16 = nullptr;  // W_n of FWHT(log) for n = 2^0..2^11 (see leo_errloc_kernel)
+    uint16_t *fold8 = nullptr;   // W_n of FWHT(log8) for n = 2^0..2^8
     ~LeoState() {
         if (device >= 0) {
             cudaFree(skew16);
             cudaFree(t16);
             cudaFree(skew8);
             cudaFree(t8);
+            cudaFree(fold16);
+            cudaFree(fold8);
         }
     }
 };
@@ -66,7 +69,7 @@ struct LeoEncArgs {
 
 struct LeoDecArgs {
     const uint8_t *shard[kLeoMaxShards];
-    uint16_t errloc[kLeoMaxRows];         // the first n error locators
+    const uint16_t *errloc;               // the first n error locators (device)
     uint32_t present[kLeoMaxShards / 32];
     uint32_t write[kLeoMaxShards / 32];   // missing shards to reveal
     int k, p, m, n, input_count;
@@ -91,13 +94,11 @@ struct F16 {
     static constexpr int kQuads = 8;
     static constexpr int kQuadShift = 3;
     using Q = uint2;
-    static __device__ __forceinline__ Q ld(const uint8_t *row, int q) {
-        return make_uint2(reinterpret_cast<const uint32_t *>(row)[q], reinterpret_cast<const uint32_t *>(row + 32)[q]);
-    }
-    static __device__ __forceinline__ void st(uint8_t *row, int q, Q v) {
-        reinterpret_cast<uint32_t *>(row)[q] = v.x;
-        reinterpret_cast<uint32_t *>(row + 32)[q] = v.y;
-    }
+    // Shared-memory rows interleave the words: quad c is (low word, high
+    // word) at byte 8c, so a warp's 8-byte loads of consecutive rows are
+    // contiguous.  Global rows keep the reference's 32 low | 32 high bytes.
+    static __device__ __forceinline__ Q ld(const uint8_t *row, int q) { return reinterpret_cast<const uint2 *>(row)[q]; }
+    static __device__ __forceinline__ void st(uint8_t *row, int q, Q v) { reinterpret_cast<uint2 *>(row)[q] = v; }
     static __device__ __forceinline__ Q ldg(const uint8_t *row, int q) {
         return make_uint2(__ldcs(reinterpret_cast<const uint32_t *>(row) + q),
                           __ldcs(reinterpret_cast<const uint32_t *>(row + 32) + q));
@@ -106,27 +107,48 @@ struct F16 {
         __stcs(reinterpret_cast<uint32_t *>(row) + q, v.x);
         __stcs(reinterpret_cast<uint32_t *>(row + 32) + q, v.y);
     }
+    // Row tile copies between the two layouts, 16 bytes (4 quads) at a time;
+    // part in [0, 2) selects quads 4*part .. 4*part+3.
+    static __device__ __forceinline__ void row_in(uint8_t *row, const uint8_t *src, int part) {
+        const uint4 lo = __ldcs(reinterpret_cast<const uint4 *>(src) + part);
+        const uint4 hi = __ldcs(reinterpret_cast<const uint4 *>(src + 32) + part);
+        reinterpret_cast<uint4 *>(row)[2 * part] = make_uint4(lo.x, hi.x, lo.y, hi.y);
+        reinterpret_cast<uint4 *>(row)[2 * part + 1] = make_uint4(lo.z, hi.z, lo.w, hi.w);
+    }
+    static __device__ __forceinline__ void row_out(uint8_t *dst, const uint8_t *row, int part) {
+        const uint4 a = reinterpret_cast<const uint4 *>(row)[2 * part];
+        const uint4 b = reinterpret_cast<const uint4 *>(row)[2 * part + 1];
+        __stcs(reinterpret_cast<uint4 *>(dst) + part, make_uint4(a.x, a.z, b.x, b.z));
+        __stcs(reinterpret_cast<uint4 *>(dst + 32) + part, make_uint4(a.y, a.w, b.y, b.w));
+    }
+    static constexpr int kRowParts = 2;
     static __device__ __forceinline__ Q zero() { return make_uint2(0, 0); }
     static __device__ __forceinline__ void xor_into(Q &a, Q b) {
         a.x ^= b.x;
         a.y ^= b.y;
     }
-    // Products by a log value lm split by symbol bits: T[0..64) covers bits
-    // 0-5, T[64..128) bits 6-11, T[128..144) bits 12-15.  Each part fits one
-    // 128-byte line, so a warp whose lanes share lm reads one line per lookup.
+    // Products by a log value lm split by symbol bits, in lm's 512-byte
+    // slot: bytes [0,128) bits 0-5, [128,256) bits 6-11, [256,288) bits 12-15.
+    // Each part fits one 128-byte line, so a warp whose lanes share lm reads
+    // one line per lookup.  Byte offsets are assembled with one PRMT each:
+    // the slot base has a zero low byte, and the low byte is 2 * index
+    // (+128 for the middle part), prepared for four symbols at once.
     const uint16_t *t;
-    static __device__ __forceinline__ uint32_t mul1(uint32_t x, const uint16_t *T) {
-        return (uint32_t)__ldg(T + (x & 63)) ^ (uint32_t)__ldg(T + 64 + ((x >> 6) & 63)) ^
-               (uint32_t)__ldg(T + 128 + ((x >> 12) & 15));
-    }
     __device__ __forceinline__ Q mul(Q v, uint32_t lm) const {
-        const uint16_t *T = t + (size_t)lm * kT16Stride;
-        // symbol i = low byte i | high byte i << 8 (bits above 15 are ignored)
-        const uint32_t r0 = mul1(__byte_perm(v.x, v.y, 0x0040), T);
-        const uint32_t r1 = mul1(__byte_perm(v.x, v.y, 0x0051), T);
-        const uint32_t r2 = mul1(__byte_perm(v.x, v.y, 0x0062), T);
-        const uint32_t r3 = mul1(__byte_perm(v.x, v.y, 0x0073), T);
-        const uint32_t r01 = __byte_perm(r0, r1, 0x5410), r23 = __byte_perm(r2, r3, 0x5410);
+        const char *T = reinterpret_cast<const char *>(t);
+        const uint32_t base = lm << 9, base2 = base + 256;
+        const uint32_t a0 = (v.x << 1) & 0x7E7E7E7Eu;
+        const uint32_t a1 = ((v.x >> 5) & 0x06060606u) | ((v.y << 3) & 0x78787878u) | 0x80808080u;
+        const uint32_t a2 = (v.y >> 3) & 0x1E1E1E1Eu;
+        uint32_t r[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const uint32_t sel = 0x7650u | (uint32_t)i;
+            r[i] = (uint32_t)__ldg(reinterpret_cast<const uint16_t *>(T + __byte_perm(a0, base, sel))) ^
+                   (uint32_t)__ldg(reinterpret_cast<const uint16_t *>(T + __byte_perm(a1, base, sel))) ^
+                   (uint32_t)__ldg(reinterpret_cast<const uint16_t *>(T + __byte_perm(a2, base2, sel)));
+        }
+        const uint32_t r01 = __byte_perm(r[0], r[1], 0x5410), r23 = __byte_perm(r[2], r[3], 0x5410);
         return make_uint2(__byte_perm(r01, r23, 0x6420), __byte_perm(r01, r23, 0x7531));
     }
 };
@@ -144,18 +166,34 @@ struct F8 {
     static __device__ __forceinline__ void stg(uint8_t *row, int q, Q v) {
         __stcs(reinterpret_cast<uint32_t *>(row) + q, v);
     }
+    static __device__ __forceinline__ void row_in(uint8_t *row, const uint8_t *src, int part) {
+        reinterpret_cast<uint4 *>(row)[part] = __ldcs(reinterpret_cast<const uint4 *>(src) + part);
+    }
+    static __device__ __forceinline__ void row_out(uint8_t *dst, const uint8_t *row, int part) {
+        __stcs(reinterpret_cast<uint4 *>(dst) + part, reinterpret_cast<const uint4 *>(row)[part]);
+    }
+    static constexpr int kRowParts = 4;
     static __device__ __forceinline__ Q zero() { return 0; }
     static __device__ __forceinline__ void xor_into(Q &a, Q b) { a ^= b; }
-    const uint8_t *t;  // shared copy of the 8 KB table: [lm][lo nibble 16 | hi nibble 16]
+    // Shared copy of the 8 KB table, 256-byte aligned: [lm][lo nibble 16 |
+    // hi nibble 16].  A lookup address is one PRMT of the prepared index
+    // byte ((lm & 7) * 32 + 16 * high + nibble) into the 256-byte block of lm.
+    uint32_t t;  // shared-space address
     __device__ __forceinline__ Q mul(Q v, uint32_t lm) const {
-        const uint8_t *T = t + lm * 32;
-        uint32_t r = 0;
+        const uint32_t blk = t + ((lm >> 3) << 8);
+        const uint32_t slot = (lm & 7u) * 0x20202020u;
+        const uint32_t lo = (v & 0x0F0F0F0Fu) | slot;
+        const uint32_t hi = ((v >> 4) & 0x0F0F0F0Fu) | slot | 0x10101010u;
+        uint32_t r[4];
 #pragma unroll
         for (int i = 0; i < 4; i++) {
-            const uint32_t b = (v >> (8 * i)) & 255u;
-            r |= (uint32_t)(T[b & 15] ^ T[16 + (b >> 4)]) << (8 * i);
+            const uint32_t sel = 0x7650u | (uint32_t)i;
+            uint32_t x, y;
+            asm volatile("ld.shared.u8 %0, [%1];" : "=r"(x) : "r"(__byte_perm(lo, blk, sel)));
+            asm volatile("ld.shared.u8 %0, [%1];" : "=r"(y) : "r"(__byte_perm(hi, blk, sel)));
+            r[i] = x ^ y;
         }
-        return r;
+        return __byte_perm(__byte_perm(r[0], r[1], 0x0040), __byte_perm(r[2], r[3], 0x0040), 0x5410);
     }
 };
 
@@ -264,14 +302,20 @@ __device__ void fft_rows(const F &f, uint8_t *w, unsigned mtrunc, unsigned m, co
     }
 }
 
-// Copies rows [first, first+cnt) of the shard list into w rows [0, cnt) and
-// zero-fills rows [cnt, rows).  16-byte vectors, 4 per row.
+// Copies rows [first, first+cnt) of the shard list into w rows [0, cnt)
+// (in the field's shared-memory layout) and zero-fills rows [cnt, rows).
+template <class F>
 __device__ void load_rows(uint8_t *w, const uint8_t *const *shard, int first, int cnt, int rows, long long off) {
-    for (int v = threadIdx.x; v < rows * 4; v += blockDim.x) {
-        const int r = v >> 2, c = v & 3;
-        uint4 x = make_uint4(0, 0, 0, 0);
-        if (r < cnt) x = __ldcs(reinterpret_cast<const uint4 *>(shard[first + r] + off) + c);
-        reinterpret_cast<uint4 *>(w + (size_t)r * kLeoTile)[c] = x;
+    for (int v = threadIdx.x; v < rows * F::kRowParts; v += blockDim.x) {
+        const int r = v / F::kRowParts, c = v % F::kRowParts;
+        uint8_t *row = w + (size_t)r * kLeoTile;
+        if (r < cnt) {
+            F::row_in(row, shard[first + r] + off, c);
+        } else {
+            constexpr int kVecs = 4 / F::kRowParts;  // 16-byte vectors per part
+#pragma unroll
+            for (int j = 0; j < kVecs; j++) reinterpret_cast<uint4 *>(row)[c * kVecs + j] = make_uint4(0, 0, 0, 0);
+        }
     }
 }
 
@@ -286,9 +330,17 @@ __device__ __forceinline__ F make_field(const uint16_t *t16, uint8_t *t8_shared)
 template <>
 __device__ __forceinline__ F16 make_field<F16>(const uint16_t *t16, uint8_t *) { return F16{t16}; }
 template <>
-__device__ __forceinline__ F8 make_field<F8>(const uint16_t *, uint8_t *t8s) { return F8{t8s}; }
+__device__ __forceinline__ F8 make_field<F8>(const uint16_t *, uint8_t *t8s) {
+    return F8{(uint32_t)__cvta_generic_to_shared(t8s)};
+}
 
 constexpr int kT8Bytes = 256 * 32;
+constexpr int kT8Slack = 256;  // the shared table starts at the next 256-byte boundary
+
+__device__ __forceinline__ uint8_t *align_shared256(uint8_t *p) {
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(p);
+    return p + ((256u - (s & 255u)) & 255u);
+}
 
 // Encode: IFFT of each m-row data block into tmp, XOR-accumulated into acc,
 // then FFT of acc; rows [0, p) of acc are the parity (leopard.go:216-270).
@@ -296,21 +348,21 @@ template <class F>
 __global__ void __launch_bounds__(kLeoThreads) leo_encode_kernel(const __grid_constant__ LeoEncArgs a) {
     extern __shared__ __align__(16) uint8_t sm[];
     const bool gf8 = F::kQuads == 16;
-    uint8_t *t8 = sm;
-    uint8_t *acc = sm + (gf8 ? kT8Bytes : 0);
+    uint8_t *t8 = gf8 ? align_shared256(sm) : sm;
+    uint8_t *acc = gf8 ? t8 + kT8Bytes : sm;
     const unsigned m = (unsigned)a.m;
     uint8_t *tmp = acc + (size_t)m * kLeoTile;
     if (gf8) load_tables8<F>(t8, a.t8);
     const F f = make_field<F>(a.t16, t8);
     const long long off = (long long)blockIdx.x * kLeoTile;
     const int cnt0 = a.k < (int)m ? a.k : (int)m;
-    load_rows(acc, a.shard, 0, cnt0, (int)m, off);
+    load_rows<F>(acc, a.shard, 0, cnt0, (int)m, off);
     __syncthreads();
     ifft_rows(f, acc, (unsigned)cnt0, m, a.skew, (int)m - 1);
     for (int b = 1; b * (int)m < a.k; b++) {
         const int start = b * (int)m;
         const int cnt = a.k - start < (int)m ? a.k - start : (int)m;
-        load_rows(tmp, a.shard, start, cnt, (int)m, off);
+        load_rows<F>(tmp, a.shard, start, cnt, (int)m, off);
         __syncthreads();
         ifft_rows(f, tmp, (unsigned)cnt, m, a.skew, (int)m - 1 + b * (int)m);
         for (int v = threadIdx.x; v < (int)m * 4; v += blockDim.x)
@@ -322,10 +374,9 @@ __global__ void __launch_bounds__(kLeoThreads) leo_encode_kernel(const __grid_co
         __syncthreads();
     }
     fft_rows(f, acc, (unsigned)a.p, m, a.skew);
-    for (int v = threadIdx.x; v < a.p * 4; v += blockDim.x) {
-        const int r = v >> 2, c = v & 3;
-        __stcs(reinterpret_cast<uint4 *>(const_cast<uint8_t *>(a.shard[a.k + r]) + off) + c,
-               reinterpret_cast<const uint4 *>(acc + (size_t)r * kLeoTile)[c]);
+    for (int v = threadIdx.x; v < a.p * F::kRowParts; v += blockDim.x) {
+        const int r = v / F::kRowParts, c = v % F::kRowParts;
+        F::row_out(const_cast<uint8_t *>(a.shard[a.k + r]) + off, acc + (size_t)r * kLeoTile, c);
     }
 }
 
@@ -360,8 +411,8 @@ template <class F>
 __global__ void __launch_bounds__(kLeoDecodeThreads) leo_decode_kernel(const __grid_constant__ LeoDecArgs a) {
     extern __shared__ __align__(16) uint8_t sm[];
     const bool gf8 = F::kQuads == 16;
-    uint8_t *t8 = sm;
-    uint8_t *w = sm + (gf8 ? kT8Bytes : 0);
+    uint8_t *t8 = gf8 ? align_shared256(sm) : sm;
+    uint8_t *w = gf8 ? t8 + kT8Bytes : sm;
     if (gf8) load_tables8<F>(t8, a.t8);
     __syncthreads();
     const F f = make_field<F>(a.t16, t8);
@@ -391,6 +442,100 @@ __global__ void __launch_bounds__(kLeoDecodeThreads) leo_decode_kernel(const __g
         const uint32_t lm = F::kMod - a.errloc[row];
         F::stg(const_cast<uint8_t *>(a.shard[i]) + off, c, f.mul(F::ld(w + (size_t)row * kLeoTile, c), lm));
     }
+}
+
+// Error locators of an erasure pattern (leopard.go:468-510,
+// leopard8.go:465-513).  The reference puts ones at erased rows (parity rows
+// first, the padding rows p..m-1, data rows at offset m), takes a 2^BITS-point
+// Walsh-Hadamard transform, multiplies by FWHT(log) mod (2^BITS - 1) and
+// transforms again, and the decoder reads only the first n = ceilPow2(m+k)
+// results.  The ones all sit below n, so the first transform is n-periodic,
+// and summing the second transform's input over the high bits leaves an
+// n-point transform: errloc[0..n) = WHT_n(WHT_n(ones) * W_n) with
+// W_n[i] = sum_h FWHT(log)[h*n + i] mod (2^BITS - 1) (built once per field).
+// The results are congruent to the reference's modulo 2^BITS - 1, which is
+// all the log-domain products that consume them depend on.
+template <int BITS>
+__device__ __forceinline__ uint32_t wh_add(uint32_t a, uint32_t b) {
+    const uint32_t s = a + b;  // partial reduction, may give the modulus (leopard.go:1001-1006)
+    return (s + (s >> BITS)) & ((1u << BITS) - 1);
+}
+template <int BITS>
+__device__ __forceinline__ uint32_t wh_sub(uint32_t a, uint32_t b) {
+    const unsigned long long d = (unsigned long long)a - (unsigned long long)b;  // wraps like Go's uint
+    return (uint32_t)((d + (d >> BITS)) & ((1u << BITS) - 1));
+}
+
+// n-point Walsh-Hadamard transform in shared memory (n a power of two).
+template <int BITS>
+__device__ void wht_shared(uint16_t *v, unsigned n) {
+    unsigned dist = 1, dist4 = 4, ld = 0;
+    for (; dist4 <= n; dist = dist4, dist4 <<= 2, ld += 2) {
+        for (unsigned it = threadIdx.x; it < (n >> 2); it += blockDim.x) {
+            const unsigned i = ((it >> ld) << (ld + 2)) + (it & (dist - 1));
+            const uint32_t t0 = v[i], t1 = v[i + dist], t2 = v[i + 2 * dist], t3 = v[i + 3 * dist];
+            const uint32_t a = wh_add<BITS>(t0, t1), b = wh_sub<BITS>(t0, t1);
+            const uint32_t c = wh_add<BITS>(t2, t3), d = wh_sub<BITS>(t2, t3);
+            v[i] = (uint16_t)wh_add<BITS>(a, c);
+            v[i + 2 * dist] = (uint16_t)wh_sub<BITS>(a, c);
+            v[i + dist] = (uint16_t)wh_add<BITS>(b, d);
+            v[i + 3 * dist] = (uint16_t)wh_sub<BITS>(b, d);
+        }
+        __syncthreads();
+    }
+    if (dist < n) {  // odd log2(n): one radix-2 layer with dist == n / 2
+        for (unsigned i = threadIdx.x; i < dist; i += blockDim.x) {
+            const uint32_t t0 = v[i], t1 = v[i + dist];
+            v[i] = (uint16_t)wh_add<BITS>(t0, t1);
+            v[i + dist] = (uint16_t)wh_sub<BITS>(t0, t1);
+        }
+        __syncthreads();
+    }
+}
+
+struct LeoErrArgs {
+    uint32_t present[kLeoMaxShards / 32];
+    int k, p, m, n;
+    const uint16_t *fold;  // W_n
+    uint16_t *out;
+};
+
+constexpr int kErrLocThreads = 512;
+
+template <int BITS>
+__global__ void __launch_bounds__(kErrLocThreads) leo_errloc_kernel(const __grid_constant__ LeoErrArgs a) {
+    constexpr uint32_t kMod = (1u << BITS) - 1;
+    __shared__ uint16_t el[kLeoMaxRows];
+    const unsigned m = (unsigned)a.m, k = (unsigned)a.k, p = (unsigned)a.p, n = (unsigned)a.n;
+    for (unsigned i = threadIdx.x; i < n; i += blockDim.x) {
+        uint16_t v = 0;
+        if (i < p) v = bit(a.present, (int)(k + i)) ? 0 : 1;
+        else if (i < m) v = 1;
+        else if (i < m + k) v = bit(a.present, (int)(i - m)) ? 0 : 1;
+        el[i] = v;
+    }
+    __syncthreads();
+    wht_shared<BITS>(el, n);
+    for (unsigned i = threadIdx.x; i < n; i += blockDim.x) el[i] = (uint16_t)(((uint32_t)el[i] * a.fold[i]) % kMod);
+    __syncthreads();
+    wht_shared<BITS>(el, n);
+    for (unsigned i = threadIdx.x; i < n; i += blockDim.x) a.out[i] = el[i];
+}
+
+// W_b for b = 0..max_bits, W_b stored at [2^b, 2^(b+1)).
+template <int BITS>
+std::vector<uint16_t> fold_walsh(const std::vector<uint16_t> &walsh, int max_bits) {
+    const unsigned order = 1u << BITS, mod = order - 1;
+    std::vector<uint16_t> out(2u << max_bits, 0);
+    for (int b = 0; b <= max_bits; b++) {
+        const unsigned n = 1u << b;
+        for (unsigned i = 0; i < n; i++) {
+            unsigned long long acc = 0;
+            for (unsigned h = 0; h < order / n; h++) acc += walsh[h * n + i];
+            out[n + i] = (uint16_t)(acc % mod);
+        }
+    }
+    return out;
 }
 
 // Builds the [65536][kT16Stride] split product tables of F16:
@@ -430,6 +575,13 @@ int ensure_tables(rsgpu_encoder *enc) {
     RS_CUDA(cudaMalloc(&st->t8, kT8Bytes));
     RS_CUDA(cudaMemcpy(st->skew16, f16.skew.data(), 65535 * 2, cudaMemcpyHostToDevice));
     RS_CUDA(cudaMemcpy(st->skew8, f8.skew.data(), 255 * 2, cudaMemcpyHostToDevice));
+    {
+        const std::vector<uint16_t> w16 = fold_walsh<16>(f16.walsh, 11), w8 = fold_walsh<8>(f8.walsh, 8);
+        RS_CUDA(cudaMalloc(&st->fold16, w16.size() * 2));
+        RS_CUDA(cudaMalloc(&st->fold8, w8.size() * 2));
+        RS_CUDA(cudaMemcpy(st->fold16, w16.data(), w16.size() * 2, cudaMemcpyHostToDevice));
+        RS_CUDA(cudaMemcpy(st->fold8, w8.data(), w8.size() * 2, cudaMemcpyHostToDevice));
+    }
     std::vector<uint8_t> t8(kT8Bytes);
     for (unsigned lm = 0; lm < 256; lm++)
         for (unsigned q = 0; q < 2; q++)
@@ -509,7 +661,7 @@ int leo_encode_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, size_t size, 
     a.skew = g16 ? enc->leo->skew16 : enc->leo->skew8;
     a.t16 = enc->leo->t16;
     a.t8 = enc->leo->t8;
-    const size_t smem = (size_t)2 * m * kLeoTile + (g16 ? 0 : kT8Bytes);
+    const size_t smem = (size_t)2 * m * kLeoTile + (g16 ? 0 : kT8Bytes + kT8Slack);
     const int grid = (int)(size / kLeoTile);
     if (!st) st = enc->ctx->stream;
     if (g16) {
@@ -570,7 +722,6 @@ int leo_reconstruct_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, const ui
     rc = ensure_tables(enc);
     if (rc) return rc;
     const bool g16 = is16(enc);
-    auto el = enc->leo->errlocs.get(g16 ? 16 : 8, k, p, present);
     static_assert(sizeof(LeoDecArgs) < 32000, "kernel parameter limit");
     auto a = std::unique_ptr<LeoDecArgs>(new LeoDecArgs());
     memset(a.get(), 0, sizeof *a);
@@ -586,7 +737,27 @@ int leo_reconstruct_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, const ui
             a->write[i >> 5] |= 1u << (i & 31);
         }
     }
-    for (unsigned r = 0; r < n; r++) a->errloc[r] = (*el)[r];
+    if (!st) st = enc->ctx->stream;
+    // error locators on the device: stream-ordered scratch, freed behind the decode
+    uint16_t *d_el = nullptr;
+    RS_CUDA(cudaMallocAsync((void **)&d_el, (size_t)n * sizeof(uint16_t), st));
+    LeoErrArgs ea;
+    memset(&ea, 0, sizeof ea);
+    memcpy(ea.present, a->present, sizeof ea.present);
+    ea.k = k;
+    ea.p = p;
+    ea.m = (int)m;
+    ea.n = (int)n;
+    ea.out = d_el;
+    ea.fold = (g16 ? enc->leo->fold16 : enc->leo->fold8) + n;
+    if (g16) leo_errloc_kernel<16><<<1, kErrLocThreads, 0, st>>>(ea);
+    else leo_errloc_kernel<8><<<1, kErrLocThreads, 0, st>>>(ea);
+    if (rc == RS_OK) rc = cuda_status(cudaGetLastError(), "leo_errloc_kernel");
+    if (rc) {
+        cudaFreeAsync(d_el, st);
+        return rc;
+    }
+    a->errloc = d_el;
     a->k = k;
     a->p = p;
     a->m = (int)m;
@@ -596,20 +767,16 @@ int leo_reconstruct_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, const ui
     a->skew = g16 ? enc->leo->skew16 : enc->leo->skew8;
     a->t16 = enc->leo->t16;
     a->t8 = enc->leo->t8;
-    const size_t smem = (size_t)n * kLeoTile + (g16 ? 0 : kT8Bytes);
+    const size_t smem = (size_t)n * kLeoTile + (g16 ? 0 : kT8Bytes + kT8Slack);
     const int grid = (int)(size / kLeoTile);
-    if (!st) st = enc->ctx->stream;
-    if (g16) {
-        rc = set_smem(leo_decode_kernel<F16>, smem);
-        if (rc) return rc;
-        leo_decode_kernel<F16><<<grid, kLeoDecodeThreads, smem, st>>>(*a);
-    } else {
-        rc = set_smem(leo_decode_kernel<F8>, smem);
-        if (rc) return rc;
-        leo_decode_kernel<F8><<<grid, kLeoDecodeThreads, smem, st>>>(*a);
+    rc = g16 ? set_smem(leo_decode_kernel<F16>, smem) : set_smem(leo_decode_kernel<F8>, smem);
+    if (rc == RS_OK) {
+        if (g16) leo_decode_kernel<F16><<<grid, kLeoDecodeThreads, smem, st>>>(*a);
+        else leo_decode_kernel<F8><<<grid, kLeoDecodeThreads, smem, st>>>(*a);
+        rc = cuda_status(cudaGetLastError(), "leo_decode_kernel");
     }
-    RS_CUDA(cudaGetLastError());
-    return RS_OK;
+    cudaFreeAsync(d_el, st);
+    return rc;
 }
 
 int leo_reconstruct(rsgpu_encoder *enc, uint8_t **shards, const uint8_t *present, size_t size,

@@ -10,11 +10,16 @@
 //     rsgpu_server_release),
 // and launches each admitted group as one micro-batch on a free stream:
 // classic stripes go into one persistent batched launch (batch.cu), Leopard
-// stripes into their fused FFT kernels.  Requests that arrive while earlier
-// micro-batches run are admitted as soon as a stream and budget free up, so
-// their work overlaps on the device.  A host callback queued behind every
-// micro-batch timestamps completion.  No device code waits on the host, so
-// nothing on the GPU can spin.
+// stripes into their fused FFT kernels.  Classic and Leopard requests queue
+// in separate lanes with their own streams, so microsecond-scale classic
+// stripes never wait behind millisecond-scale Leopard stripes: the classic
+// lane runs on high-priority streams and may use the whole byte budget
+// except what Leopard work holds, while the Leopard lane is held to three
+// quarters of it.  Requests that arrive while earlier micro-batches run are
+// admitted as soon as a stream and budget free up, so their work overlaps
+// on the device.  Host callbacks queued behind every micro-batch (and behind
+// every Leopard stripe) timestamp completion.  No device code waits on the
+// host, so nothing on the GPU can spin.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -32,8 +37,12 @@ using Clock = std::chrono::steady_clock;
 namespace rsgpu {
 namespace {
 
+constexpr int kLanes = 2;          // 0: classic stripes, 1: Leopard stripes
+constexpr int kLeoPerSlot = 2;     // Leopard stripes per micro-batch (each is a full-GPU launch)
+
 struct Req {
     uint64_t ticket = 0;
+    int lane = 0;
     rsgpu_request *user = nullptr;  // output pointers are written back here
     rsgpu_request r{};
     std::vector<uint8_t *> shards;
@@ -43,9 +52,12 @@ struct Req {
     int status = RS_OK;
     int verify_slot = -1;
     Clock::time_point t_submit, t_done;
+    std::atomic<int64_t> t_kernel_done{0};  // set by a host callback (Leopard stripes)
 };
 
 struct Slot {
+    rsgpu_server *sv = nullptr;
+    int lane = 0;
     cudaStream_t stream = nullptr;
     rsgpu_batch *batch = nullptr;
     std::vector<Req *> reqs;
@@ -117,11 +129,11 @@ struct rsgpu_server {
 
     std::mutex mu;  // guards everything below
     std::condition_variable cv;
-    std::deque<Req *> queue;         // submitted, not admitted
+    std::deque<Req *> queue[kLanes]; // submitted, not admitted
     std::map<uint64_t, Req *> live;  // admitted or done, not yet polled/released
     std::deque<Req *> done;          // completed, not yet polled
     uint64_t next_ticket = 1;
-    size_t inflight = 0;
+    size_t inflight[kLanes] = {0, 0};
     bool stop = false;
     std::thread worker;
 
@@ -143,6 +155,24 @@ void CUDART_CB on_slot_done(void *arg) {
     auto *s = static_cast<Slot *>(arg);
     s->t_done = Clock::now();
     s->finished.store(true, std::memory_order_release);
+    s->sv->cv.notify_all();
+}
+
+void CUDART_CB on_req_done(void *arg) {
+    auto *q = static_cast<Req *>(arg);
+    q->t_kernel_done.store(Clock::now().time_since_epoch().count(), std::memory_order_release);
+}
+
+bool queues_empty(const rsgpu_server *sv) {
+    for (int l = 0; l < kLanes; l++)
+        if (!sv->queue[l].empty()) return false;
+    return true;
+}
+
+size_t total_inflight(const rsgpu_server *sv) {
+    size_t t = 0;
+    for (int l = 0; l < kLanes; l++) t += sv->inflight[l];
+    return t;
 }
 
 int encoder_for(rsgpu_server *sv, const rsgpu_request &r, rsgpu_encoder **out) {
@@ -205,15 +235,20 @@ void finish(rsgpu_server *sv, Req *q, Clock::time_point t) {
 // number admitted.
 int admit(rsgpu_server *sv, Slot *s) {
     int n = 0;
-    while (!sv->queue.empty() && n < sv->max_batch) {
-        Req *q = sv->queue.front();
+    auto &queue = sv->queue[s->lane];
+    const int max_n = s->lane == 1 ? std::min(sv->max_batch, kLeoPerSlot) : sv->max_batch;
+    const size_t cap = s->lane == 1 ? sv->inflight_budget - sv->inflight_budget / 4
+                                    : sv->inflight_budget - std::min(sv->inflight_budget, sv->inflight[1]);
+    size_t &inflight = sv->inflight[s->lane];
+    while (!queue.empty() && n < max_n) {
+        Req *q = queue.front();
         rsgpu_encoder *e = nullptr;
         int rc = encoder_for(sv, q->r, &e);
         std::vector<int> outs;
         if (rc == RS_OK && (q->r.op == RS_JOB_RECONSTRUCT || q->r.op == RS_JOB_RECONSTRUCT_DATA))
             rc = outputs_of(sv, q, e, outs);
         if (rc != RS_OK) {  // fails immediately, no device work
-            sv->queue.pop_front();
+            queue.pop_front();
             q->status = rc;
             finish(sv, q, Clock::now());
             continue;
@@ -231,7 +266,7 @@ int admit(rsgpu_server *sv, Slot *s) {
             }
             fp = (reads + outs.size()) * sz;
         }
-        if (sv->inflight > 0 && sv->inflight + fp > sv->inflight_budget) break;
+        if (inflight > 0 && inflight + fp > cap) break;
         // reconstruct outputs without a caller buffer come from the arena
         std::vector<size_t> offs;
         bool ok = true;
@@ -249,8 +284,8 @@ int admit(rsgpu_server *sv, Slot *s) {
             for (size_t off : offs) sv->arena.release(off);
             for (int o : outs)
                 if (q->user && !q->user->shards[o]) q->shards[o] = nullptr;
-            if (n == 0 && sv->inflight == 0 && sv->arena.used.empty()) {
-                sv->queue.pop_front();  // can never fit
+            if (n == 0 && total_inflight(sv) == 0 && sv->arena.used.empty()) {
+                queue.pop_front();  // can never fit
                 q->status = RS_ERR_NOMEM;
                 finish(sv, q, Clock::now());
                 continue;
@@ -259,9 +294,9 @@ int admit(rsgpu_server *sv, Slot *s) {
         }
         q->arena_off = offs;
         q->footprint = fp;
-        sv->queue.pop_front();
-        sv->inflight += fp;
-        sv->max_inflight = std::max(sv->max_inflight, sv->inflight);
+        queue.pop_front();
+        inflight += fp;
+        sv->max_inflight = std::max(sv->max_inflight, total_inflight(sv));
         s->reqs.push_back(q);
         n++;
     }
@@ -312,6 +347,7 @@ void launch(rsgpu_server *sv, Slot *s) {
             rc = leo_reconstruct_enqueue(e, q->shards.data(), q->present.data(), q->r.shard_size,
                                          q->r.op == RS_JOB_RECONSTRUCT, st);
         if (rc) q->status = rc;
+        else if (cudaLaunchHostFunc(st, on_req_done, q) != cudaSuccess) q->t_kernel_done.store(0);
     }
     s->finished.store(false);
     s->busy = true;
@@ -337,8 +373,9 @@ void reap(rsgpu_server *sv, Slot *s) {
             q->user->result = (q->verify_slot >= 0 && q->verify_slot < (int)ok.size()) ? ok[q->verify_slot] : 0;
         if (q->user)
             for (size_t i = 0; i < q->shards.size(); i++) q->user->shards[i] = q->shards[i];
-        sv->inflight -= q->footprint;
-        finish(sv, q, s->t_done);
+        sv->inflight[q->lane] -= q->footprint;
+        const int64_t t = q->t_kernel_done.load(std::memory_order_acquire);
+        finish(sv, q, t ? Clock::time_point(Clock::duration(t)) : s->t_done);
     }
     s->reqs.clear();
     s->busy = false;
@@ -354,13 +391,13 @@ void worker_loop(rsgpu_server *sv) {
                 reap(sv, s);
                 progress = true;
             }
-        if (sv->stop && sv->queue.empty()) {
+        if (sv->stop && queues_empty(sv)) {
             bool busy = false;
             for (Slot *s : sv->slots) busy |= s->busy;
             if (!busy) break;
         }
         for (Slot *s : sv->slots) {
-            if (s->busy || sv->queue.empty()) continue;
+            if (s->busy || sv->queue[s->lane].empty()) continue;
             if (admit(sv, s) > 0) {
                 launch(sv, s);
                 progress = true;
@@ -393,12 +430,17 @@ int rsgpu_server_create(rsgpu_ctx *ctx, size_t arena_bytes, size_t inflight_budg
         }
     }
     sv->arena.init(arena_bytes);
-    for (int i = 0; i < streams; i++) {
-        auto *s = new Slot();
-        cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
-        rsgpu_batch_create(ctx, nullptr, &s->batch);
-        sv->slots.push_back(s);
-    }
+    int prio_low = 0, prio_high = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+    for (int lane = 0; lane < kLanes; lane++)
+        for (int i = 0; i < streams; i++) {
+            auto *s = new Slot();
+            s->sv = sv;
+            s->lane = lane;
+            cudaStreamCreateWithPriority(&s->stream, cudaStreamNonBlocking, lane == 0 ? prio_high : prio_low);
+            rsgpu_batch_create(ctx, nullptr, &s->batch);
+            sv->slots.push_back(s);
+        }
     sv->worker = std::thread(worker_loop, sv);
     *out = sv;
     return RS_OK;
@@ -412,6 +454,7 @@ int rsgpu_server_submit(rsgpu_server *sv, rsgpu_request *r, uint64_t *ticket) {
     auto *q = new Req();
     q->user = r;
     q->r = *r;
+    q->lane = r->leopard ? 1 : 0;
     q->shards.assign(r->shards, r->shards + n);
     if (r->present) q->present.assign(r->present, r->present + n);
     else q->present.assign(n, 1);
@@ -424,7 +467,7 @@ int rsgpu_server_submit(rsgpu_server *sv, rsgpu_request *r, uint64_t *ticket) {
         }
         q->ticket = sv->next_ticket++;
         sv->live[q->ticket] = q;
-        sv->queue.push_back(q);
+        sv->queue[q->lane].push_back(q);
         sv->n_submitted++;
         if (!sv->any) {
             sv->any = true;
@@ -472,11 +515,11 @@ int rsgpu_server_wait_idle(rsgpu_server *sv, int timeout_ms) {
     std::unique_lock<std::mutex> lk(sv->mu);
     const auto deadline = Clock::now() + std::chrono::milliseconds(timeout_ms);
     while (true) {
-        bool busy = !sv->queue.empty();
+        bool busy = !queues_empty(sv);
         for (Slot *s : sv->slots) busy |= s->busy;
         if (!busy) return RS_OK;
         if (sv->cv.wait_until(lk, deadline) == std::cv_status::timeout) {
-            busy = !sv->queue.empty();
+            busy = !queues_empty(sv);
             for (Slot *s : sv->slots) busy |= s->busy;
             return busy ? RS_ERR_TIMEOUT : RS_OK;
         }
@@ -512,7 +555,7 @@ int rsgpu_server_reset_stats(rsgpu_server *sv) {
     std::lock_guard<std::mutex> lk(sv->mu);
     sv->n_submitted = sv->n_completed = sv->n_failed = 0;
     sv->bytes_done = 0;
-    sv->max_inflight = sv->inflight;
+    sv->max_inflight = total_inflight(sv);
     sv->latencies_us.clear();
     sv->any = false;
     return RS_OK;
