@@ -8,9 +8,6 @@ namespace rsgpu {
 namespace gf8dev {
 
 constexpr int kThreads = 256;
-#ifndef FIXED_MINB
-#define FIXED_MINB 1
-#endif
 constexpr int kHalfStride = 256;         // bytes between the tables of one (input, half)
 constexpr int kInStride = 2 * kHalfStride;
 constexpr int kTableAlign = 256;         // table base alignment in the shared window
@@ -73,6 +70,12 @@ __device__ __forceinline__ uint32_t mulhi(uint32_t a, uint32_t b) {
     return r;
 }
 
+__device__ __forceinline__ uint32_t madhi(uint32_t a, uint32_t b, uint32_t c) {
+    uint32_t r;
+    asm("mad.hi.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c));
+    return r;
+}
+
 struct Mul {
     uint32_t m[8];
 };
@@ -98,13 +101,15 @@ __device__ __forceinline__ void nibble_addrs(uint32_t x, uint32_t lb, uint32_t h
         h[3] = (mulhi(x, mu.m[7]) & 0x3Cu) | hb;
     } else {
         // bytes of lo4/hi4 are 4*nibble; PRMT drops byte j into the (zero)
-        // low byte of the 256-aligned table base.
+        // low byte of the 256-aligned table base.  Byte 3 goes through the
+        // FMA pipe instead (hi32(v * 256) + base), which takes a quarter of
+        // the address work off the integer ALU pipe.
         const uint32_t lo4 = (x * mu.m[0]) & 0x3C3C3C3Cu;
         const uint32_t hi4 = mulhi(x, mu.m[4]) & 0x3C3C3C3Cu;
         l[0] = __byte_perm(lo4, lb, 0x7650); h[0] = __byte_perm(hi4, hb, 0x7650);
         l[1] = __byte_perm(lo4, lb, 0x7651); h[1] = __byte_perm(hi4, hb, 0x7651);
         l[2] = __byte_perm(lo4, lb, 0x7652); h[2] = __byte_perm(hi4, hb, 0x7652);
-        l[3] = __byte_perm(lo4, lb, 0x7653); h[3] = __byte_perm(hi4, hb, 0x7653);
+        l[3] = madhi(lo4, 256u, lb);         h[3] = madhi(hi4, 256u, hb);
     }
 }
 

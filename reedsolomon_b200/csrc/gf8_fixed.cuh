@@ -1,0 +1,138 @@
+// gf8_fixed.cuh -- input-count-specialised GF(2^8) contraction kernels.
+//
+// The unrolled kernel is instantiated once per register floor (MINB = the
+// resident CTAs per SM the allocator must allow) in its own translation
+// unit (kernels_gf8_fixed{1,2,3,4}.cu), so the four variants compile in
+// parallel.  MINB 1 lets the unrolled loop keep ~160 registers (8 warps per
+// SM), 2 caps it at 128, 3 at 80, 4 at 64; the autotuner times them.
+#pragma once
+
+#include "gf8_device.cuh"
+#include "kernels.h"
+
+namespace rsgpu {
+
+typedef void (*VecKernel)(GfMatArgs);
+
+// The specialised kernel for (n_in, output groups G, mode), or nullptr when
+// n_in has no specialisation (4, 5, 6, 8, 10, 12, 16, 17, 20 do) or G > 2.
+VecKernel fixed_kernel_minb1(int n_in, int G, int mode);
+VecKernel fixed_kernel_minb2(int n_in, int G, int mode);
+VecKernel fixed_kernel_minb3(int n_in, int G, int mode);
+VecKernel fixed_kernel_minb4(int n_in, int G, int mode);
+
+#ifdef RSGPU_FIXED_MINB
+namespace {
+
+using namespace gf8dev;
+
+// Input-count-specialised kernel: the input loop is fully unrolled, so table
+// offsets are immediates and no per-input guards remain; batch b+1's loads
+// are issued before batch b is multiplied, and the next vector's first batch
+// before the outputs are stored.
+template <int N, int G, int MODE, int V, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB) gf8_matmul_fixed(const __grid_constant__ GfMatArgs a) {
+    extern __shared__ __align__(128) uint32_t smem_raw[];
+    uint32_t *tab = aligned_tables(smem_raw);
+    constexpr int NB = (N + 3) / 4;
+    const long long nvec = a.nbytes >> 4;
+    const long long stride = (long long)gridDim.x * kThreads;
+    long long v = (long long)blockIdx.x * kThreads + threadIdx.x;
+    uint4 nx[4] = {};
+    if (v < nvec) {
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            if (j < N) nx[j] = ld_in(a.in[j], v);
+    }
+    build_tables<G>(tab, a);
+    Mul mu;
+#pragma unroll
+    for (int j = 0; j < 8; j++) mu.m[j] = a.mul[j];
+    __syncthreads();
+    const uint32_t tab_s = (uint32_t)__cvta_generic_to_shared(tab);
+    uint32_t mism = 0;
+    for (; v < nvec; v += stride) {
+        uint32_t acc[G][16];
+#pragma unroll
+        for (int g = 0; g < G; g++)
+#pragma unroll
+            for (int b = 0; b < 16; b++) acc[g][b] = 0;
+#pragma unroll
+        for (int b = 0; b < NB; b++) {
+            uint4 cur[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) cur[j] = nx[j];
+            if (b + 1 < NB) {
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                    if (4 * (b + 1) + j < N) nx[j] = ld_in(a.in[4 * (b + 1) + j], v);
+            } else if (v + stride < nvec) {
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                    if (j < N) nx[j] = ld_in(a.in[j], v + stride);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (4 * b + j < N) mac_vec<G, V>(cur[j], tab_s + (4 * b + j) * kInStride, mu, acc);
+        }
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+            uint4 w[4];
+            transpose4x4(acc[g][0], acc[g][1], acc[g][2], acc[g][3], w[0].x, w[1].x, w[2].x, w[3].x);
+            transpose4x4(acc[g][4], acc[g][5], acc[g][6], acc[g][7], w[0].y, w[1].y, w[2].y, w[3].y);
+            transpose4x4(acc[g][8], acc[g][9], acc[g][10], acc[g][11], w[0].z, w[1].z, w[2].z, w[3].z);
+            transpose4x4(acc[g][12], acc[g][13], acc[g][14], acc[g][15], w[0].w, w[1].w, w[2].w, w[3].w);
+#pragma unroll
+            for (int o = 0; o < 4; o++) {
+                const int oo = 4 * g + o;
+                if (oo >= a.n_out) break;
+                uint4 *dst = reinterpret_cast<uint4 *>(a.out[oo]) + v;
+                if (MODE == kModeWrite) {
+                    __stcs(dst, w[o]);
+                } else if (MODE == kModeXor) {
+                    uint4 old = __ldcs(dst);
+                    old.x ^= w[o].x; old.y ^= w[o].y; old.z ^= w[o].z; old.w ^= w[o].w;
+                    __stcs(dst, old);
+                } else {
+                    const uint4 chk = __ldcs(dst);
+                    mism |= (chk.x ^ w[o].x) | (chk.y ^ w[o].y) | (chk.z ^ w[o].z) | (chk.w ^ w[o].w);
+                }
+            }
+        }
+    }
+    if (MODE == kModeVerify && mism) *reinterpret_cast<volatile int *>(a.flag) = 1;
+}
+
+template <int N, int G>
+VecKernel pick_fixed(int mode) {
+    if (mode == kModeWrite) return gf8_matmul_fixed<N, G, kModeWrite, kVariantPrmt, RSGPU_FIXED_MINB>;
+    if (mode == kModeXor) return gf8_matmul_fixed<N, G, kModeXor, kVariantPrmt, RSGPU_FIXED_MINB>;
+    return gf8_matmul_fixed<N, G, kModeVerify, kVariantPrmt, RSGPU_FIXED_MINB>;
+}
+
+template <int G>
+VecKernel fixed_for_g(int n_in, int mode) {
+    switch (n_in) {
+    case 4: return pick_fixed<4, G>(mode);
+    case 5: return pick_fixed<5, G>(mode);
+    case 6: return pick_fixed<6, G>(mode);
+    case 8: return pick_fixed<8, G>(mode);
+    case 10: return pick_fixed<10, G>(mode);
+    case 12: return pick_fixed<12, G>(mode);
+    case 16: return pick_fixed<16, G>(mode);
+    case 17: return pick_fixed<17, G>(mode);
+    case 20: return pick_fixed<20, G>(mode);
+    }
+    return nullptr;
+}
+
+VecKernel fixed_for(int n_in, int G, int mode) {
+    if (G == 1) return fixed_for_g<1>(n_in, mode);
+    if (G == 2) return fixed_for_g<2>(n_in, mode);
+    return nullptr;
+}
+
+}  // namespace
+#endif  // RSGPU_FIXED_MINB
+
+}  // namespace rsgpu

@@ -42,7 +42,8 @@ enum GfVariant : int {
     kVariantFixed = 3,  // PRMT addressing, input loop unrolled for the exact input count
     kVariantFixed2 = 4, // as kVariantFixed, registers capped for 2 resident CTAs per SM
     kVariantFixed3 = 5, // as kVariantFixed, registers capped for 3 resident CTAs per SM
-    kNumVariants = 6,
+    kVariantFixed4 = 6, // as kVariantFixed, registers capped for 4 resident CTAs per SM
+    kNumVariants = 7,
 };
 
 // Force a variant for every launch (-1 restores the tuned / default choice).

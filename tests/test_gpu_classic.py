@@ -291,7 +291,7 @@ def test_rs10x4_64mib_roundtrip_and_windows():
             assert torch.equal(cp[int(i)], orig[int(i)])
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6])
 def test_every_kernel_variant_bit_exact(variant):
     """Each nibble-address variant of the GF(2^8) kernel gives the oracle's bytes."""
     lib = rs.lib()
