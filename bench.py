@@ -146,6 +146,22 @@ def cpu_reference(seconds, threads, shard=SHARD, max_steps=None):
     return k * shard * n / el / 1e9, n, el, isa
 
 
+def max_over_ranks(x, world, device):
+    """The slowest rank's value (device-timed milliseconds) on every rank."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def stripe_seed(rank):
+    """Each rank encodes its own stripe (independent data, weak scaling)."""
+    return 1000 + rank
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -181,7 +197,6 @@ def run_e2e(args, enc, lib, shards, S, stream, dev, world, barrier):
     """Encode through the host-buffer C-ABI entry point; every step moves the
     data shards H2D from pinned memory and the parity D2H."""
     import torch
-    import torch.distributed as dist
     import reedsolomon_b200 as rs
     k, p = K_DATA, P_PARITY
     hs = [torch.empty(S, dtype=torch.uint8, pin_memory=True) for _ in range(k + p)]
@@ -199,11 +214,7 @@ def run_e2e(args, enc, lib, shards, S, stream, dev, world, barrier):
         rs.encoder.check(lib.rsgpu_encode_host(enc._h, hptrs, S))
     e1.record(stream)
     barrier()
-    ems = e0.elapsed_time(e1)
-    if world > 1:
-        tt = torch.tensor([ems], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ems = float(tt.item())
+    ems = max_over_ranks(e0.elapsed_time(e1), world, dev)
     for i in range(k, k + p):
         assert torch.equal(hs[i].to(dev), shards[i]), "host-path parity differs from device path"
     return world * k * S / (ems / e2e_steps / 1e3) / 1e9
@@ -469,7 +480,7 @@ def run_ours(args):
 
     dev = torch.device("cuda", local)
     k, p, S = K_DATA, P_PARITY, args.shard_mib << 20
-    g = torch.Generator(device=dev).manual_seed(1000 + rank)
+    g = torch.Generator(device=dev).manual_seed(stripe_seed(rank))
     shards = [torch.randint(0, 256, (S,), dtype=torch.uint8, device=dev, generator=g) for _ in range(k)]
     shards += [torch.empty(S, dtype=torch.uint8, device=dev) for _ in range(p)]
     enc = rs.New(k, p, rs.WithGPU(local))
@@ -515,11 +526,7 @@ def run_ours(args):
             step()
         t1.record(stream)
         barrier()
-    ms = t0.elapsed_time(t1)
-    if world > 1:
-        tt = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = max_over_ranks(t0.elapsed_time(t1), world, dev)
     ms_step = ms / args.steps
     value = world * k * S / (ms_step / 1e3) / 1e9
     peak, peak_kind = peaks()
@@ -531,7 +538,7 @@ def run_ours(args):
         e2e = run_e2e(args, enc, lib, shards, S, stream, dev, world, barrier)
 
     extras = None
-    if not args.no_extras:
+    if not args.no_extras and world == 1:  # secondary legs: single-GPU runs only
         want = set(args.extras.split(","))
         extras = {}
         if "verify" in want:
@@ -567,7 +574,7 @@ def run_ours(args):
             "extras": extras,
             "clocks": clk.summary(),
         }
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and world == 1:  # rank 0 at N=1 only
             threads = os.cpu_count() or 1
             gbs, n, el, isa = cpu_reference(args.cpu_seconds, threads, shard=16 << 20)
             out["cpu_baseline"] = {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": "port",
