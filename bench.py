@@ -49,7 +49,7 @@ def parse():
                     help="shard size; the headline workload is 64 MiB")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the secondary measurements (verify, reconstruct, batch, leopard)")
-    ap.add_argument("--extras", default="verify,reconstruct,batch,leopard,serving",
+    ap.add_argument("--extras", default="verify,reconstruct,progressive,batch,leopard,serving",
                     help="comma list of secondary measurements to run")
     ap.add_argument("--batch-stripes", type=int, default=4096)
     ap.add_argument("--variant", type=int, default=-1,
@@ -368,6 +368,48 @@ def extra_leopard(dev):
     return out
 
 
+def extra_progressive(enc, shards, S, reps=5):
+    """Update of 2 of the 10 data shards and a 4-erasure DecodeIdx fed in two
+    progressive calls, on the RS(10,4) x 64 MiB stripe (copies, so the
+    headline buffers stay intact)."""
+    import torch
+    k, p = K_DATA, P_PARITY
+    stream = torch.cuda.current_stream()
+    work = [s.clone() for s in shards]
+    new = [None] * k
+    new[2], new[7] = shards[0].clone(), shards[1].clone()
+    enc.Update(work, new)  # warm
+    a, b = _ev(), _ev()
+    a.record(stream)
+    for _ in range(reps):
+        enc.Update(work, new)
+    b.record(stream)
+    b.synchronize()
+    ms_u = a.elapsed_time(b) / reps
+    lost = (1, 4, 10, 12)
+    expect = [0 if i in lost else 1 for i in range(k + p)]
+    dst = [torch.zeros(S, dtype=torch.uint8, device=shards[0].device) if i in lost else None for i in range(k + p)]
+    avail = [i for i in range(k + p) if expect[i]]
+    batches = (avail[:5], avail[5:])
+    ms_d = []
+    for _ in range(reps + 1):
+        for d in dst:
+            if d is not None:
+                d.zero_()
+        a, b = _ev(), _ev()
+        a.record(stream)
+        for batch in batches:
+            enc.DecodeIdx(dst, expect, [shards[i] if i in batch else None for i in range(k + p)])
+        b.record(stream)
+        b.synchronize()
+        ms_d.append(a.elapsed_time(b))
+    ok = all(torch.equal(dst[i], shards[i]) for i in lost)
+    del work
+    return {"update_2_of_10_ms": round(ms_u, 4), "update_changed_GBps": round(2 * S / (ms_u / 1e3) / 1e9, 1),
+            "decode_idx_4_lost_2_calls_ms": round(min(ms_d[1:]), 4),
+            "decode_idx_data_GBps": round(k * S / (min(ms_d[1:]) / 1e3) / 1e9, 1), "decode_idx_bit_exact": ok}
+
+
 SERVE_GEOS = ((6, 3, 0), (10, 4, 0), (17, 3, 0), (1000, 200, 1))  # (k, p, leopard GF(2^16))
 SERVE_MAX = 4 << 20
 
@@ -549,6 +591,8 @@ def run_ours(args):
             extras["batch"] = extra_batch(dev, args.batch_stripes)
         if "leopard" in want:
             extras["leopard"] = extra_leopard(dev)
+        if "progressive" in want:
+            extras["progressive"] = extra_progressive(enc, shards, S)
         if "serving" in want:
             extras["serving"] = extra_serving(dev)
     out = None

@@ -120,6 +120,19 @@ int rsgpu_encode(rsgpu_encoder *enc, uint8_t *const *shards, size_t shard_size);
 /* EncodeIdx (reedsolomon.go:708-757): parity[o] ^= M[k+o][idx] * data */
 int rsgpu_encode_idx(rsgpu_encoder *enc, const uint8_t *data_shard, int idx, uint8_t *const *parity,
                      size_t shard_size);
+/* Update (reedsolomon.go:762-853): for every data shard c with new_data[c]
+ * != NULL, shards[c] ^= new_data[c] (like the reference, the old shard is left
+ * holding the delta) and parity ^= P[:, c] * delta.  Leopard: ErrNotSupported
+ * (leopard.go:316). */
+int rsgpu_update(rsgpu_encoder *enc, uint8_t *const *shards, const uint8_t *const *new_data,
+                 size_t shard_size);
+/* DecodeIdx (reedsolomon.go:1464-1617): progressive decoding.  expect[k+p]
+ * marks the shards that will arrive as input; input[i] (NULL when not in this
+ * call) contributes to every non-NULL dst[j] through the decode matrix of the
+ * first k expected shards, accumulated (dst must start zeroed).  expect ==
+ * NULL: merging mode, dst[i] ^= input[i].  Leopard: ErrNotSupported. */
+int rsgpu_decode_idx(rsgpu_encoder *enc, uint8_t *const *dst, const uint8_t *expect,
+                     const uint8_t *const *input, size_t shard_size);
 /* Verify (reedsolomon.go:857-871; leopard.go:393-419) */
 int rsgpu_verify(rsgpu_encoder *enc, uint8_t *const *shards, size_t shard_size, int *ok);
 /* Reconstruct / ReconstructData / ReconstructSome (reedsolomon.go:1446,1634,1655;

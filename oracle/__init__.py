@@ -28,6 +28,8 @@ _SIGS = {
     "ora_code_some_shards": (None, [c_voidp, c_int, c_int, c_voidp, c_voidp, c_size, c_int]),
     "ora_rs_encode": (c_int, [c_int, c_int, c_int, c_voidp, c_size]),
     "ora_rs_encode_idx": (c_int, [c_int, c_int, c_int, c_voidp, c_int, c_voidp, c_size]),
+    "ora_rs_update": (c_int, [c_int, c_int, c_int, c_voidp, c_voidp, c_size]),
+    "ora_rs_decode_idx": (c_int, [c_int, c_int, c_int, c_voidp, c_voidp, c_voidp, c_size]),
     "ora_rs_verify": (c_int, [c_int, c_int, c_int, c_voidp, c_size, ctypes.POINTER(c_int)]),
     "ora_rs_reconstruct": (c_int, [c_int, c_int, c_int, c_voidp, c_voidp, c_size, c_int, c_voidp, c_int, c_voidp]),
     "ora_rs_decode_rows": (c_int, [c_int, c_int, c_int, c_voidp, c_int, c_voidp, c_int, c_voidp, c_voidp,
@@ -50,6 +52,10 @@ _SIGS = {
 }
 
 MAT = {"default": 0, "cauchy": 1, "par1": 2, "jerasure": 3, "xor": 4}
+# status codes of oracle.h (the reference's sentinel errors)
+ERR = {"too_few_shards": -1, "shard_no_data": -2, "shard_size": -3, "invalid_shard_size": -4,
+       "inv_shard_num": -5, "max_shard_num": -6, "not_supported": -7, "invalid_input": -8,
+       "singular": -10, "not_square": -11}
 
 
 def lib():
@@ -145,6 +151,17 @@ def rs_encode(k, p, shards, kind="default"):
 
 def rs_encode_idx(k, p, data, idx, parity, kind="default"):
     return lib().ora_rs_encode_idx(k, p, MAT[kind], data.ctypes.data, idx, _rows_ptrs(parity), len(data))
+
+
+def rs_update(k, p, shards, new_data, size, kind="default"):
+    """Update (reedsolomon.go:762-853) in place; None entries are absent shards."""
+    return lib().ora_rs_update(k, p, MAT[kind], _rows_ptrs(shards), _rows_ptrs(new_data), size)
+
+
+def rs_decode_idx(k, p, dst, expect, inputs, size, kind="default"):
+    """DecodeIdx (reedsolomon.go:1464-1617); expect=None selects merging mode."""
+    return lib().ora_rs_decode_idx(k, p, MAT[kind], _rows_ptrs(dst), _u8(expect) if expect is not None else None,
+                                   _rows_ptrs(inputs), size)
 
 
 def rs_verify(k, p, shards, kind="default"):

@@ -432,6 +432,93 @@ int ora_rs_reconstruct(int k, int p, int kind, uint8_t *const *shards, const uin
     return rc;
 }
 
+/* reedsolomon.go:762-853 Update / updateParityShards: for every data shard c
+ * with new data, old[c] ^= new[c] (the reference overwrites the old shard
+ * with the delta), then parity[o] ^= M[k+o][c] * old[c]. */
+int ora_rs_update(int k, int p, int kind, uint8_t *const *shards, const uint8_t *const *new_data,
+                  size_t size) {
+    if (size == 0) return ORA_ERR_SHARD_NO_DATA;
+    int any = 0;
+    for (int i = 0; i < k; i++) {
+        if (new_data[i]) {
+            any = 1;
+            if (!shards[i]) return ORA_ERR_INVALID_INPUT;
+        }
+    }
+    if (!any) return ORA_ERR_SHARD_NO_DATA;
+    for (int o = 0; o < p; o++)
+        if (!shards[k + o]) return ORA_ERR_INVALID_INPUT;
+    if (p == 0) return ORA_OK;
+    uint8_t *m;
+    int rc = classic_matrix(k, p, kind, &m);
+    if (rc) return rc;
+    for (int c = 0; c < k; c++) {
+        if (!new_data[c]) continue;
+        for (size_t j = 0; j < size; j++) shards[c][j] ^= new_data[c][j];
+        for (int o = 0; o < p; o++) ora_gal_mul_slice(m[(size_t)(k + o) * k + c], shards[c], shards[k + o], size, 1);
+    }
+    free(m);
+    return ORA_OK;
+}
+
+/* reedsolomon.go:1464-1617 DecodeIdx.  expect == NULL: merging mode, dst[i]
+ * ^= input[i].  Otherwise the decode matrix of the first k expected shards
+ * (inverse of their encoding rows), one row per non-NULL dst (data rows from
+ * the inverse, parity rows as parity row x inverse), restricted to the
+ * columns whose input is present in this call, accumulated into dst. */
+int ora_rs_decode_idx(int k, int p, int kind, uint8_t *const *dst, const uint8_t *expect,
+                      const uint8_t *const *input, size_t size) {
+    const int total = k + p;
+    if (!expect) {
+        for (int i = 0; i < total; i++)
+            if (input[i] && !dst[i]) return ORA_ERR_INVALID_INPUT;
+        for (int i = 0; i < total; i++)
+            if (input[i])
+                for (size_t j = 0; j < size; j++) dst[i][j] ^= input[i][j];
+        return ORA_OK;
+    }
+    for (int i = 0; i < total; i++)
+        if (input[i] && !expect[i]) return ORA_ERR_INVALID_INPUT;
+    for (int i = 0; i < total; i++)
+        if (expect[i] && dst[i]) return ORA_ERR_INVALID_INPUT;
+    int *valid = (int *)malloc(sizeof(int) * (size_t)total);
+    int nv = 0;
+    for (int i = 0; i < total; i++)
+        if (expect[i]) valid[nv++] = i;
+    if (nv < k) {
+        free(valid);
+        return ORA_ERR_TOO_FEW_SHARDS;
+    }
+    uint8_t *m;
+    int rc = classic_matrix(k, p, kind, &m);
+    if (rc) {
+        free(valid);
+        return rc;
+    }
+    uint8_t *subm = (uint8_t *)malloc((size_t)k * k), *dec = (uint8_t *)malloc((size_t)k * k);
+    for (int r = 0; r < k; r++) memcpy(subm + (size_t)r * k, m + (size_t)valid[r] * k, k);
+    rc = ora_mat_invert(subm, k, dec);
+    if (rc == ORA_OK) {
+        uint8_t *row = (uint8_t *)malloc((size_t)k);
+        for (int d = 0; d < total; d++) {
+            if (!dst[d]) continue;
+            if (d < k) memcpy(row, dec + (size_t)d * k, k);
+            else row_times_matrix(m + (size_t)d * k, dec, k, row);
+            /* columns beyond the first k valid shards carry zero coefficients */
+            for (int col = 0; col < k; col++) {
+                const uint8_t *in = input[valid[col]];
+                if (in) ora_gal_mul_slice(row[col], in, dst[d], size, 1);
+            }
+        }
+        free(row);
+    }
+    free(subm);
+    free(dec);
+    free(m);
+    free(valid);
+    return rc;
+}
+
 /* ------------------------------------------------------------------------ */
 /* Leopard GF(2^16) (leopard.go)                                               */
 /* ------------------------------------------------------------------------ */

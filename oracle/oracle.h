@@ -70,6 +70,10 @@ int ora_rs_verify(int k, int p, int kind, uint8_t *const *shards, size_t size, i
 int ora_rs_reconstruct(int k, int p, int kind, uint8_t *const *shards, const uint8_t *present,
                        size_t size, int data_only, const uint8_t *required, int n_required,
                        uint8_t *written);
+int ora_rs_update(int k, int p, int kind, uint8_t *const *shards, const uint8_t *const *new_data,
+                  size_t size);
+int ora_rs_decode_idx(int k, int p, int kind, uint8_t *const *dst, const uint8_t *expect,
+                      const uint8_t *const *input, size_t size);
 int ora_rs_decode_rows(int k, int p, int kind, const uint8_t *present, int data_only,
                        const uint8_t *required, int n_required, uint8_t *rows_out,
                        int *out_idx, int *n_out, int *in_idx);

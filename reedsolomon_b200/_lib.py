@@ -104,6 +104,8 @@ SIGNATURES = {
     "rsgpu_autotune_gf8": (c_int, [c_voidp, c_int, c_int, c_size, c_int, c_int, c_voidp, c_intp]),
     "rsgpu_force_variant": (c_int, [c_int]),
     "rsgpu_num_variants": (c_int, []),
+    "rsgpu_update": (c_int, [c_voidp, c_voidp, c_voidp, c_size]),
+    "rsgpu_decode_idx": (c_int, [c_voidp, c_voidp, c_voidp, c_voidp, c_size]),
     "rsgpu_batch_create": (c_int, [c_voidp, c_voidp, ctypes.POINTER(c_voidp)]),
     "rsgpu_batch_destroy": (c_int, [c_voidp]),
     "rsgpu_batch_clear": (c_int, [c_voidp]),

@@ -475,6 +475,110 @@ int rsgpu_encode_idx(rsgpu_encoder *enc, const uint8_t *data, int idx, uint8_t *
     return sync(enc->ctx);
 }
 
+int rsgpu_update(rsgpu_encoder *enc, uint8_t *const *shards, const uint8_t *const *new_data, size_t size) {
+    NEED_CTX(enc);
+    if (enc->codec != RS_CODEC_CLASSIC) return RS_ERR_NOT_SUPPORTED;  // leopard.go:316, leopard8.go:289
+    if (!shards || !new_data) return RS_ERR_TOO_FEW_SHARDS;
+    std::lock_guard<std::recursive_mutex> lk(enc->ctx->mu);
+    if (size == 0) return RS_ERR_SHARD_NO_DATA;
+    const int k = enc->k, p = enc->p;
+    std::vector<int> cols;
+    for (int c = 0; c < k; c++)
+        if (new_data[c]) {
+            if (!shards[c]) return RS_ERR_INVALID_INPUT;
+            cols.push_back(c);
+        }
+    if (cols.empty()) return RS_ERR_SHARD_NO_DATA;  // checkShards(newDatashards, true)
+    for (int o = 0; o < p; o++)
+        if (!shards[k + o]) return RS_ERR_INVALID_INPUT;
+    if (p == 0) return RS_OK;  // updateParityShards returns before touching the data
+    // old[c] ^= new[c] (the reference leaves the delta in the old shard), then
+    // parity ^= P[:, cols] * delta in one accumulating contraction.
+    const int n = (int)cols.size();
+    std::vector<const uint8_t *> ins(n);
+    std::vector<uint8_t> rows((size_t)p * n);
+    for (int j = 0; j < n; j++) {
+        RS_CUDA(launch_xor(enc->ctx->stream, enc->ctx->info, new_data[cols[j]], shards[cols[j]], size));
+        ins[j] = shards[cols[j]];
+        for (int o = 0; o < p; o++) rows[(size_t)o * n + j] = enc->parity_rows[(size_t)o * k + cols[j]];
+    }
+    int rc = run_matmul(enc->ctx, rows.data(), n, p, ins.data(), shards + k, size, kModeXor);
+    if (rc) return rc;
+    return sync(enc->ctx);
+}
+
+int rsgpu_decode_idx(rsgpu_encoder *enc, uint8_t *const *dst, const uint8_t *expect,
+                     const uint8_t *const *input, size_t size) {
+    NEED_CTX(enc);
+    if (enc->codec != RS_CODEC_CLASSIC) return RS_ERR_NOT_SUPPORTED;  // leopard.go:94, leopard8.go:90
+    if (!dst || !input) return RS_ERR_INVALID_INPUT;
+    std::lock_guard<std::recursive_mutex> lk(enc->ctx->mu);
+    const int k = enc->k, total = enc->total;
+    if (!expect) {  // merging mode: dst[i] ^= input[i]
+        for (int i = 0; i < total; i++)
+            if (input[i] && !dst[i]) return RS_ERR_INVALID_INPUT;
+        if (size == 0) return RS_OK;
+        for (int i = 0; i < total; i++)
+            if (input[i]) RS_CUDA(launch_xor(enc->ctx->stream, enc->ctx->info, input[i], dst[i], size));
+        return sync(enc->ctx);
+    }
+    for (int i = 0; i < total; i++) {
+        if (input[i] && !expect[i]) return RS_ERR_INVALID_INPUT;  // unexpected input
+        if (expect[i] && dst[i]) return RS_ERR_INVALID_INPUT;     // dst of an expected input
+    }
+    std::vector<int> valid, invalid;
+    for (int i = 0; i < total; i++) (expect[i] ? valid : invalid).push_back(i);
+    if ((int)valid.size() < k) return RS_ERR_TOO_FEW_SHARDS;
+    // getDecodeMatrix (reedsolomon.go:634-673): inverse of the first k
+    // expected rows, cached in the inversion tree under the unexpected set.
+    std::shared_ptr<const Matrix> dec;
+    if (enc->tree) dec = enc->tree->get(invalid);
+    if (!dec) {
+        Matrix sub(k, k);
+        for (int r = 0; r < k; r++)
+            for (int c = 0; c < k; c++) sub.at(r, c) = enc->m.at(valid[r], c);
+        auto inv = std::make_shared<Matrix>();
+        int rc = mat_invert(sub, *inv);
+        if (rc) return rc;
+        dec = inv;
+        if (enc->tree) enc->tree->insert(invalid, inv);
+    }
+    // inputs present in this call; columns past the first k expected shards
+    // carry zero coefficients and are skipped
+    std::vector<int> cols;
+    for (int col = 0; col < k; col++)
+        if (input[valid[col]]) cols.push_back(col);
+    std::vector<int> outs;
+    for (int d = 0; d < total; d++)
+        if (dst[d]) outs.push_back(d);
+    if (cols.empty() || outs.empty() || size == 0) return RS_OK;
+    const Gf256 &g = Gf256::get();
+    const int n_in = (int)cols.size(), n_out = (int)outs.size();
+    std::vector<uint8_t> rows((size_t)n_out * n_in);
+    std::vector<uint8_t> full(k);
+    for (int o = 0; o < n_out; o++) {
+        const int d = outs[o];
+        if (d < k) {
+            for (int c = 0; c < k; c++) full[c] = dec->at(d, c);
+        } else {
+            const uint8_t *pr = enc->m.row(d);
+            for (int c = 0; c < k; c++) {
+                uint8_t v = 0;
+                for (int t = 0; t < k; t++) v ^= g.mul[pr[t]][dec->at(t, c)];
+                full[c] = v;
+            }
+        }
+        for (int j = 0; j < n_in; j++) rows[(size_t)o * n_in + j] = full[cols[j]];
+    }
+    std::vector<const uint8_t *> ins(n_in);
+    std::vector<uint8_t *> dsts(n_out);
+    for (int j = 0; j < n_in; j++) ins[j] = input[valid[cols[j]]];
+    for (int o = 0; o < n_out; o++) dsts[o] = dst[outs[o]];
+    int rc = run_matmul(enc->ctx, rows.data(), n_in, n_out, ins.data(), dsts.data(), size, kModeXor);
+    if (rc) return rc;
+    return sync(enc->ctx);
+}
+
 int rsgpu_verify(rsgpu_encoder *enc, uint8_t *const *shards, size_t size, int *ok) {
     NEED_CTX(enc);
     if (!ok) return RS_ERR_INVALID_INPUT;

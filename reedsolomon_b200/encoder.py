@@ -270,6 +270,94 @@ class Encoder:
         check(L.lib().rsgpu_encode_idx(self._h, _ptr(data_shard), idx,
                                        L.ptr_array([_ptr(p) for p in parity]), size))
 
+    def Update(self, shards, newDatashards):
+        """Update (reedsolomon.go:762-853): parity += P * (old ^ new) for every
+        data shard with new data; the old data shard is left holding old ^ new,
+        as in the reference.  Device shards only."""
+        if self.codec != RS_CODEC_CLASSIC:
+            raise ErrNotSupported("operation not supported")
+        if len(shards) != self.TotalShards() or len(newDatashards) != self._k:
+            raise ErrTooFewShards("too few shards given")
+        size, dev = self._prep(shards, nilok=True)
+        nsize = _size(newDatashards)
+        if nsize == 0:
+            raise ErrShardNoData("no shard data")
+        for s in newDatashards:
+            n = 0 if s is None else len(s)
+            if n != nsize and n != 0:
+                raise ErrShardSize("shard sizes do not match")
+        for i, s in enumerate(newDatashards):
+            if s is not None and len(s) and (shards[i] is None or not len(shards[i])):
+                raise ErrInvalidInput("invalid input")
+        if any(p is None or not len(p) for p in shards[self._k:]):
+            raise ErrInvalidInput("invalid input")
+        if nsize != size:  # the reference would index past the shorter slices
+            raise ErrShardSize("shard sizes do not match")
+        if not dev or not all(_is_device(s) for s in newDatashards if s is not None and len(s)):
+            raise ErrNotSupported("Update takes device shards")
+        self._bind()
+        new = [s if (s is not None and len(s)) else None for s in newDatashards]
+        check(L.lib().rsgpu_update(self._h, L.ptr_array([_ptr(s) for s in shards]),
+                                   L.ptr_array([_ptr(s) for s in new]), size))
+
+    def DecodeIdx(self, dst, expectInput, input):
+        """DecodeIdx (reedsolomon.go:1464-1617): accumulate this call's inputs
+        into the non-None dst shards (zeroed by the caller before the first
+        call); expectInput=None merges two partial results (dst ^= input)."""
+        if self.codec != RS_CODEC_CLASSIC:
+            raise ErrNotSupported("operation not supported")
+        lib = L.lib()
+        if expectInput is None:
+            if len(dst) != len(input):
+                raise ErrInvalidInput("dst and input must have same length for merging")
+            for i, x in enumerate(input):
+                if x is not None:
+                    if dst[i] is None:
+                        raise ErrInvalidInput("input[%d] provided but dst[%d] is nil" % (i, i))
+                    if len(dst[i]) != len(x):
+                        raise ErrInvalidShardSize("dst[%d] size != input[%d] size" % (i, i))
+            pad = [None] * (self.TotalShards() - 1)
+            for i, x in enumerate(input):  # pairs may differ in size: one merge call per pair
+                if x is not None and len(x):
+                    self._device_only([x, dst[i]])
+                    self._bind()
+                    check(lib.rsgpu_decode_idx(self._h, L.ptr_array([_ptr(dst[i])] + pad), None,
+                                               L.ptr_array([_ptr(x)] + pad), len(x)))
+            return
+        n = self.TotalShards()
+        if len(expectInput) != n or len(dst) != n or len(input) != n:
+            raise ErrInvalidInput("expectInput, dst and input must have totalShards entries")
+        for i in range(n):
+            if input[i] is not None and not expectInput[i]:
+                raise ErrInvalidInput("unexpected input at index %d" % i)
+            if expectInput[i] and dst[i] is not None:
+                raise ErrInvalidInput("dst[%d] should be nil" % i)
+        if sum(1 for e in expectInput if e) < self._k:
+            raise ErrTooFewShards("too few shards given")
+        size = 0
+        for x in input:
+            if x is not None:
+                if size == 0:
+                    size = len(x)
+                elif len(x) != size:
+                    raise ErrInvalidShardSize("input sizes differ")
+        for d in dst:
+            if d is not None and len(d) != size:
+                raise ErrInvalidShardSize("dst size differs from the input size")
+        live = [x for x in list(dst) + list(input) if x is not None and len(x)]
+        if not live:
+            return
+        self._device_only(live)
+        self._bind()
+        check(lib.rsgpu_decode_idx(self._h, L.ptr_array([_ptr(d) for d in dst]),
+                                   L.u8_array([1 if e else 0 for e in expectInput]),
+                                   L.ptr_array([_ptr(x) for x in input]), size))
+
+    @staticmethod
+    def _device_only(tensors):
+        if not all(_is_device(t) for t in tensors):
+            raise ErrNotSupported("takes device shards")
+
     def Verify(self, shards):
         size, dev = self._prep(shards, nilok=False)
         if not dev:

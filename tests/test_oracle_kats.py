@@ -154,3 +154,44 @@ def test_oracle_leopard8_rejects_overlong_geometry():
     # 200+56: ceilPow2(56)+200 > 256 indexes past the reference's tables (leopard8.go:151,441)
     sh = [np.zeros(64, np.uint8) for _ in range(256)]
     assert O.leo_encode(8, 200, 56, sh) == -6
+
+
+def test_oracle_update_and_decode_idx_properties():
+    """Update (reedsolomon.go:762-853) leaves parity equal to a fresh encode of
+    the new data and the delta in the old shard; DecodeIdx
+    (reedsolomon.go:1464-1617) fed progressively, and merged, rebuilds the
+    shards a Reconstruct would."""
+    rng = np.random.default_rng(11)
+    k, p, S = 7, 4, 333
+    sh = [rng.integers(0, 256, S, dtype=np.uint8) for _ in range(k)] + [np.zeros(S, np.uint8) for _ in range(p)]
+    assert O.rs_encode(k, p, sh) == 0
+    new = [None] * k
+    for c in (0, 3, 6):
+        new[c] = rng.integers(0, 256, S, dtype=np.uint8)
+    upd = [a.copy() for a in sh]
+    assert O.rs_update(k, p, upd, new, S) == 0
+    fresh = [a.copy() for a in sh]
+    for c in (0, 3, 6):
+        fresh[c] = new[c].copy()
+    assert O.rs_encode(k, p, fresh) == 0
+    for i in range(k, k + p):
+        assert np.array_equal(upd[i], fresh[i])
+    for c in (0, 3, 6):
+        assert np.array_equal(upd[c], sh[c] ^ new[c])
+    assert O.rs_update(k, p, upd, [None] * k, S) == O.ERR["shard_no_data"]
+    # progressive decode in three calls, two of them merged from a second dst set
+    expect = [1, 0, 1, 1, 0, 1, 1, 1, 0, 1, 0]
+    dst_a = [None if e else np.zeros(S, np.uint8) for e in expect]
+    dst_b = [None if e else np.zeros(S, np.uint8) for e in expect]
+    for batch, dst in (([0, 2], dst_a), ([3, 5], dst_b), ([6, 7, 9], dst_a)):
+        inp = [sh[i] if i in batch else None for i in range(k + p)]
+        assert O.rs_decode_idx(k, p, dst, expect, inp, S) == 0
+    assert O.rs_decode_idx(k, p, dst_a, None, dst_b, S) == 0
+    for i in range(k + p):
+        if dst_a[i] is not None:
+            assert np.array_equal(dst_a[i], sh[i]), i
+    bad = [None] * (k + p)
+    bad[1] = sh[1]
+    assert O.rs_decode_idx(k, p, dst_a, expect, bad, S) == O.ERR["invalid_input"]
+    few = [1, 1, 1] + [0] * (k + p - 3)
+    assert O.rs_decode_idx(k, p, [None] * (k + p), few, [None] * (k + p), S) == O.ERR["too_few_shards"]
