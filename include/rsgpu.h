@@ -44,6 +44,7 @@ extern "C" {
 #define RS_ERR_RECONSTRUCT_REQUIRED -9  /* ErrReconstructRequired reedsolomon.go:1862 */
 #define RS_ERR_SINGULAR -10             /* errSingular          matrix.go:184 */
 #define RS_ERR_NOT_SQUARE -11           /* errNotSquare         matrix.go:187 */
+#define RS_ERR_SHORT_DATA -12           /* ErrShortData         reedsolomon.go:1785 */
 #define RS_ERR_CUDA -100                /* a CUDA call failed (see rsgpu_last_error) */
 #define RS_ERR_NOMEM -101               /* device or pinned allocation failed */
 #define RS_ERR_TIMEOUT -102             /* a bounded device wait expired */
@@ -133,6 +134,20 @@ int rsgpu_update(rsgpu_encoder *enc, uint8_t *const *shards, const uint8_t *cons
  * NULL: merging mode, dst[i] ^= input[i].  Leopard: ErrNotSupported. */
 int rsgpu_decode_idx(rsgpu_encoder *enc, uint8_t *const *dst, const uint8_t *expect,
                      const uint8_t *const *input, size_t shard_size);
+/* Split (reedsolomon.go:1803-1856; leopard.go:320-370) of `len` bytes of
+ * device data into k+p shards of *per_shard = ceil(len/k) bytes (Leopard:
+ * rounded up to 64).  data[len, cap) may be used as spare room, like a Go
+ * slice's capacity, and is zeroed.  rsgpu_split_plan gives per_shard and the
+ * bytes of padding the split needs; rsgpu_split fills shards[k+p] with views
+ * of `data` for the shards that fit and, for the rest, zeroed 64-byte aligned
+ * slices of the caller's `padding` buffer (64-byte aligned, padding_bytes
+ * long), into which the data past the last full shard is copied. */
+int rsgpu_split_plan(rsgpu_encoder *enc, size_t len, size_t cap, size_t *per_shard, size_t *padding_bytes);
+int rsgpu_split(rsgpu_encoder *enc, uint8_t *data, size_t len, size_t cap, uint8_t *padding,
+                size_t padding_bytes, uint8_t **shards, size_t *per_shard);
+/* Join (reedsolomon.go:1858-1898): copies the first out_size bytes of the
+ * data shards (device, shard_size bytes each) to dst (device or host). */
+int rsgpu_join(rsgpu_encoder *enc, void *dst, uint8_t *const *shards, size_t shard_size, size_t out_size);
 /* Verify (reedsolomon.go:857-871; leopard.go:393-419) */
 int rsgpu_verify(rsgpu_encoder *enc, uint8_t *const *shards, size_t shard_size, int *ok);
 /* Reconstruct / ReconstructData / ReconstructSome (reedsolomon.go:1446,1634,1655;

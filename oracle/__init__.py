@@ -29,6 +29,8 @@ _SIGS = {
     "ora_rs_encode": (c_int, [c_int, c_int, c_int, c_voidp, c_size]),
     "ora_rs_encode_idx": (c_int, [c_int, c_int, c_int, c_voidp, c_int, c_voidp, c_size]),
     "ora_rs_update": (c_int, [c_int, c_int, c_int, c_voidp, c_voidp, c_size]),
+    "ora_split": (c_int, [c_int, c_int, c_int, c_voidp, c_size, c_voidp, c_voidp]),
+    "ora_join": (c_int, [c_int, c_voidp, c_voidp, c_int, c_voidp, c_size]),
     "ora_rs_decode_idx": (c_int, [c_int, c_int, c_int, c_voidp, c_voidp, c_voidp, c_size]),
     "ora_rs_verify": (c_int, [c_int, c_int, c_int, c_voidp, c_size, ctypes.POINTER(c_int)]),
     "ora_rs_reconstruct": (c_int, [c_int, c_int, c_int, c_voidp, c_voidp, c_size, c_int, c_voidp, c_int, c_voidp]),
@@ -55,7 +57,7 @@ MAT = {"default": 0, "cauchy": 1, "par1": 2, "jerasure": 3, "xor": 4}
 # status codes of oracle.h (the reference's sentinel errors)
 ERR = {"too_few_shards": -1, "shard_no_data": -2, "shard_size": -3, "invalid_shard_size": -4,
        "inv_shard_num": -5, "max_shard_num": -6, "not_supported": -7, "invalid_input": -8,
-       "singular": -10, "not_square": -11}
+       "reconstruct_required": -9, "singular": -10, "not_square": -11, "short_data": -12}
 
 
 def lib():
@@ -151,6 +153,25 @@ def rs_encode(k, p, shards, kind="default"):
 
 def rs_encode_idx(k, p, data, idx, parity, kind="default"):
     return lib().ora_rs_encode_idx(k, p, MAT[kind], data.ctypes.data, idx, _rows_ptrs(parity), len(data))
+
+
+def split(k, p, data, leopard=False):
+    """Split (reedsolomon.go:1803-1856, leopard.go:320-370): (rc, list of k+p shards)."""
+    per = ctypes.c_size_t()
+    rc = lib().ora_split(k, p, int(leopard), data.ctypes.data if len(data) else None, len(data), ctypes.byref(per), None)
+    if rc:
+        return rc, None
+    out = np.zeros((k + p) * per.value, np.uint8)
+    lib().ora_split(k, p, int(leopard), data.ctypes.data, len(data), ctypes.byref(per), out.ctypes.data)
+    return 0, [out[i * per.value:(i + 1) * per.value] for i in range(k + p)]
+
+
+def join(k, shards, out_size):
+    """Join (reedsolomon.go:1858-1898): (rc, bytes)."""
+    sizes = (ctypes.c_size_t * max(1, len(shards)))(*[0 if s is None else len(s) for s in shards])
+    dst = np.zeros(max(1, out_size), np.uint8)
+    rc = lib().ora_join(k, _rows_ptrs(shards), sizes, len(shards), dst.ctypes.data, out_size)
+    return rc, (dst[:out_size] if rc == 0 else None)
 
 
 def rs_update(k, p, shards, new_data, size, kind="default"):

@@ -519,6 +519,45 @@ int ora_rs_decode_idx(int k, int p, int kind, uint8_t *const *dst, const uint8_t
     return rc;
 }
 
+/* reedsolomon.go:1803-1856 Split / leopard.go:320-370 (leopard: per-shard
+ * size rounded up to 64): writes the k+p shards, each per_shard bytes, one
+ * after the other into out (total * per_shard bytes).  `cap` >= len models the
+ * slice capacity the reference reuses (its bytes past len are zeroed); the
+ * content of the shards does not depend on where each one lives. */
+int ora_split(int k, int p, int leopard, const uint8_t *data, size_t len, size_t *per_shard, uint8_t *out) {
+    const int total = k + p;
+    if (len == 0) return ORA_ERR_SHORT_DATA;
+    size_t per = (len + (size_t)k - 1) / (size_t)k;
+    if (leopard) per = (per + 63) / 64 * 64;
+    if (total == 1 && (!leopard || (len & 63) == 0)) per = len;
+    *per_shard = per;
+    if (!out) return ORA_OK;
+    memset(out, 0, per * (size_t)total);
+    memcpy(out, data, len);
+    return ORA_OK;
+}
+
+/* reedsolomon.go:1858-1898 Join: the first out_size bytes of the data shards. */
+int ora_join(int k, const uint8_t *const *shards, const size_t *sizes, int n_shards, uint8_t *dst,
+             size_t out_size) {
+    if (n_shards < k) return ORA_ERR_TOO_FEW_SHARDS;
+    size_t have = 0;
+    for (int i = 0; i < k; i++) {
+        if (!shards[i]) return ORA_ERR_RECONSTRUCT_REQUIRED;
+        have += sizes[i];
+        if (have >= out_size) break;
+    }
+    if (have < out_size) return ORA_ERR_SHORT_DATA;
+    size_t write = out_size, off = 0;
+    for (int i = 0; i < k && write; i++) {
+        const size_t n = write < sizes[i] ? write : sizes[i];
+        memcpy(dst + off, shards[i], n);
+        off += n;
+        write -= n;
+    }
+    return ORA_OK;
+}
+
 /* ------------------------------------------------------------------------ */
 /* Leopard GF(2^16) (leopard.go)                                               */
 /* ------------------------------------------------------------------------ */

@@ -34,8 +34,10 @@ enum {
     ORA_ERR_MAX_SHARD_NUM = -6,
     ORA_ERR_NOT_SUPPORTED = -7,
     ORA_ERR_INVALID_INPUT = -8,
+    ORA_ERR_RECONSTRUCT_REQUIRED = -9,
     ORA_ERR_SINGULAR = -10,
     ORA_ERR_NOT_SQUARE = -11,
+    ORA_ERR_SHORT_DATA = -12,
 };
 
 /* matrix kinds (options.go:252-303 WithJerasureMatrix / WithPAR1Matrix / WithCauchyMatrix / WithFastOneParityMatrix) */
@@ -70,6 +72,9 @@ int ora_rs_verify(int k, int p, int kind, uint8_t *const *shards, size_t size, i
 int ora_rs_reconstruct(int k, int p, int kind, uint8_t *const *shards, const uint8_t *present,
                        size_t size, int data_only, const uint8_t *required, int n_required,
                        uint8_t *written);
+int ora_split(int k, int p, int leopard, const uint8_t *data, size_t len, size_t *per_shard, uint8_t *out);
+int ora_join(int k, const uint8_t *const *shards, const size_t *sizes, int n_shards, uint8_t *dst,
+             size_t out_size);
 int ora_rs_update(int k, int p, int kind, uint8_t *const *shards, const uint8_t *const *new_data,
                   size_t size);
 int ora_rs_decode_idx(int k, int p, int kind, uint8_t *const *dst, const uint8_t *expect,

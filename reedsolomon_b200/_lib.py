@@ -105,6 +105,9 @@ SIGNATURES = {
     "rsgpu_force_variant": (c_int, [c_int]),
     "rsgpu_num_variants": (c_int, []),
     "rsgpu_update": (c_int, [c_voidp, c_voidp, c_voidp, c_size]),
+    "rsgpu_split_plan": (c_int, [c_voidp, c_size, c_size, c_voidp, c_voidp]),
+    "rsgpu_split": (c_int, [c_voidp, c_voidp, c_size, c_size, c_voidp, c_size, c_voidp, c_voidp]),
+    "rsgpu_join": (c_int, [c_voidp, c_voidp, c_voidp, c_size, c_size]),
     "rsgpu_decode_idx": (c_int, [c_voidp, c_voidp, c_voidp, c_voidp, c_size]),
     "rsgpu_batch_create": (c_int, [c_voidp, c_voidp, ctypes.POINTER(c_voidp)]),
     "rsgpu_batch_destroy": (c_int, [c_voidp]),

@@ -215,6 +215,7 @@ const char *rsgpu_status_string(int s) {
     case RS_ERR_RECONSTRUCT_REQUIRED: return "reconstruction required as one or more required data shards are nil";
     case RS_ERR_SINGULAR: return "matrix is singular";
     case RS_ERR_NOT_SQUARE: return "only square matrices can be inverted";
+    case RS_ERR_SHORT_DATA: return "not enough data to fill the number of requested shards";
     case RS_ERR_CUDA: return "CUDA error";
     case RS_ERR_NOMEM: return "out of device memory";
     case RS_ERR_TIMEOUT: return "device wait timed out";
@@ -472,6 +473,99 @@ int rsgpu_encode_idx(rsgpu_encoder *enc, const uint8_t *data, int idx, uint8_t *
     for (int o = 0; o < enc->p; o++) col[o] = enc->parity_rows[(size_t)o * enc->k + idx];
     rc = run_matmul(enc->ctx, col.data(), 1, enc->p, &data, parity, size, kModeXor);
     if (rc) return rc;
+    return sync(enc->ctx);
+}
+
+// Split layout shared by rsgpu_split_plan and rsgpu_split.
+struct SplitLayout {
+    size_t per = 0, usable = 0, pitch = 0, padding = 0;
+    int full = 0;  // shards that are views of the caller's data
+};
+
+static int split_layout(const rsgpu_encoder *enc, size_t len, size_t cap, SplitLayout &L) {
+    if (len == 0) return RS_ERR_SHORT_DATA;
+    const bool leo = enc->codec != RS_CODEC_CLASSIC;
+    const size_t total = (size_t)enc->total;
+    if (cap < len) cap = len;
+    if (total == 1 && (!leo || (len & 63) == 0)) {  // a single shard is the data itself
+        L.per = len;
+        L.usable = len;
+        L.full = 1;
+        return RS_OK;
+    }
+    L.per = (len + (size_t)enc->k - 1) / (size_t)enc->k;
+    if (leo) L.per = (L.per + 63) / 64 * 64;
+    const size_t need = total * L.per;
+    L.usable = cap > len ? std::min(cap, need) : len;
+    if (L.usable < need) {
+        L.full = (int)(L.usable / L.per);
+        L.pitch = (L.per + 63) & ~(size_t)63;  // AllocAligned (unsafe.go:19-43)
+        L.padding = L.pitch * (total - (size_t)L.full);
+    } else {
+        L.full = (int)total;
+    }
+    return RS_OK;
+}
+
+int rsgpu_split_plan(rsgpu_encoder *enc, size_t len, size_t cap, size_t *per_shard, size_t *padding_bytes) {
+    if (!enc || !per_shard || !padding_bytes) return RS_ERR_INVALID_INPUT;
+    SplitLayout L;
+    int rc = split_layout(enc, len, cap, L);
+    if (rc) return rc;
+    *per_shard = L.per;
+    *padding_bytes = L.padding;
+    return RS_OK;
+}
+
+int rsgpu_split(rsgpu_encoder *enc, uint8_t *data, size_t len, size_t cap, uint8_t *padding,
+                size_t padding_bytes, uint8_t **shards, size_t *per_shard) {
+    NEED_CTX(enc);
+    if (!shards || !per_shard) return RS_ERR_INVALID_INPUT;
+    SplitLayout L;
+    int rc = split_layout(enc, len, cap, L);
+    if (rc) return rc;
+    if (!data) return RS_ERR_INVALID_INPUT;
+    if (L.padding && (!padding || padding_bytes < L.padding || ((uintptr_t)padding & 63))) return RS_ERR_INVALID_INPUT;
+    std::lock_guard<std::recursive_mutex> lk(enc->ctx->mu);
+    cudaStream_t st = enc->ctx->stream;
+    if (L.usable > len) RS_CUDA(cudaMemsetAsync(data + len, 0, L.usable - len, st));  // clear(data[dataLen:])
+    for (int i = 0; i < L.full; i++) shards[i] = data + (size_t)i * L.per;
+    if (L.padding) {
+        RS_CUDA(cudaMemsetAsync(padding, 0, L.padding, st));
+        // the bytes past the last full shard go to the first padding shards
+        size_t from = (size_t)L.full * L.per;
+        for (int i = L.full; i < enc->total; i++) {
+            shards[i] = padding + (size_t)(i - L.full) * L.pitch;
+            if (from < len) {
+                const size_t n = std::min(L.per, len - from);
+                RS_CUDA(cudaMemcpyAsync(shards[i], data + from, n, cudaMemcpyDeviceToDevice, st));
+                from += n;
+            }
+        }
+    }
+    *per_shard = L.per;
+    return sync(enc->ctx);
+}
+
+int rsgpu_join(rsgpu_encoder *enc, void *dst, uint8_t *const *shards, size_t shard_size, size_t out_size) {
+    NEED_CTX(enc);
+    if (!shards) return RS_ERR_TOO_FEW_SHARDS;
+    size_t have = 0;
+    for (int i = 0; i < enc->k; i++) {
+        if (!shards[i]) return RS_ERR_RECONSTRUCT_REQUIRED;
+        have += shard_size;
+        if (have >= out_size) break;
+    }
+    if (have < out_size) return RS_ERR_SHORT_DATA;
+    if (out_size && !dst) return RS_ERR_INVALID_INPUT;
+    std::lock_guard<std::recursive_mutex> lk(enc->ctx->mu);
+    size_t write = out_size, off = 0;
+    for (int i = 0; i < enc->k && write; i++) {
+        const size_t n = std::min(write, shard_size);
+        RS_CUDA(cudaMemcpyAsync((uint8_t *)dst + off, shards[i], n, cudaMemcpyDefault, enc->ctx->stream));
+        off += n;
+        write -= n;
+    }
     return sync(enc->ctx);
 }
 

@@ -41,13 +41,14 @@ ErrInvalidInput = _err("ErrInvalidInput", -8)
 ErrReconstructRequired = _err("ErrReconstructRequired", -9)
 ErrSingular = _err("ErrSingular", -10)
 ErrNotSquare = _err("ErrNotSquare", -11)
+ErrShortData = _err("ErrShortData", -12)
 CudaError = _err("CudaError", -100)
 ErrNoMem = _err("ErrNoMem", -101)
 ErrTimeout = _err("ErrTimeout", -102)
 ErrNoDevice = _err("ErrNoDevice", -103)
 _BY_CODE = {c.code: c for c in (ErrTooFewShards, ErrShardNoData, ErrShardSize, ErrInvalidShardSize,
                                 ErrInvShardNum, ErrMaxShardNum, ErrNotSupported, ErrInvalidInput,
-                                ErrReconstructRequired, ErrSingular, ErrNotSquare, CudaError, ErrNoMem,
+                                ErrReconstructRequired, ErrSingular, ErrNotSquare, ErrShortData, CudaError, ErrNoMem,
                                 ErrTimeout, ErrNoDevice)}
 
 
@@ -357,6 +358,78 @@ class Encoder:
     def _device_only(tensors):
         if not all(_is_device(t) for t in tensors):
             raise ErrNotSupported("takes device shards")
+
+    def Split(self, data):
+        """Split (reedsolomon.go:1803-1856; leopard.go:320-370) of a 1-D uint8
+        CUDA tensor into k+p shards of ceil(len/k) bytes (Leopard: rounded up
+        to 64).  Full shards are views of `data`; the rest share one zeroed
+        padding buffer."""
+        return self.SplitCap(data, len(data), len(data))
+
+    def SplitCap(self, buf, length, cap):
+        """Split of buf[:length] with buf[length:cap] usable as spare capacity,
+        as the reference uses a slice's capacity (those bytes are zeroed)."""
+        if not _is_device(buf) or buf.dtype != torch.uint8 or not buf.is_contiguous():
+            raise ErrNotSupported("Split takes a contiguous uint8 device tensor")
+        cap = max(int(cap), int(length))
+        if cap > buf.numel():
+            raise ErrInvalidInput("cap exceeds the buffer")
+        lib = L.lib()
+        per, pad = ctypes.c_size_t(), ctypes.c_size_t()
+        check(lib.rsgpu_split_plan(self._h, int(length), cap, ctypes.byref(per), ctypes.byref(pad)))
+        padding = torch.empty(pad.value + 64, dtype=torch.uint8, device=buf.device) if pad.value else None
+        pad_off = 0
+        if padding is not None:
+            pad_off = (-padding.data_ptr()) % 64
+        ptrs = L.ptr_array([None] * self.TotalShards())
+        self._bind()
+        check(lib.rsgpu_split(self._h, _ptr(buf) if length else None, int(length), cap,
+                              None if padding is None else ctypes.c_void_p(padding.data_ptr() + pad_off),
+                              pad.value, ptrs, ctypes.byref(per)))
+        out = []
+        base, pbase = buf.data_ptr(), (padding.data_ptr() + pad_off) if padding is not None else None
+        for i in range(self.TotalShards()):
+            addr = ptrs[i]
+            if base <= addr < base + cap:
+                out.append(buf[addr - base:addr - base + per.value])
+            else:
+                off = addr - pbase
+                out.append(padding[pad_off + off:pad_off + off + per.value])
+        return out
+
+    def Join(self, dst, shards, outSize):
+        """Join (reedsolomon.go:1858-1898): the first outSize bytes of the data
+        shards into `dst` (a uint8 tensor, device or host, of >= outSize bytes,
+        or an object with write())."""
+        if len(shards) < self._k:
+            raise ErrTooFewShards("too few shards given")
+        have = 0
+        for s in shards[:self._k]:
+            if s is None:
+                raise ErrReconstructRequired("reconstruction required")
+            have += len(s)
+            if have >= outSize:
+                break
+        if have < outSize:
+            raise ErrShortData("not enough data to fill the number of requested shards")
+        sizes = {len(s) for s in shards[:self._k] if s is not None}
+        if len(sizes) > 1:
+            raise ErrShardSize("shard sizes do not match")
+        size = sizes.pop()
+        lib = L.lib()
+        data = [s if (s is not None) else None for s in shards[:self._k]] + [None] * self._p
+        if isinstance(dst, torch.Tensor):
+            if dst.numel() < outSize or dst.dtype != torch.uint8 or not dst.is_contiguous():
+                raise ErrShortData("dst is shorter than outSize")
+            self._bind()
+            check(lib.rsgpu_join(self._h, ctypes.c_void_p(dst.data_ptr()), L.ptr_array([_ptr(s) for s in data]),
+                                 size, int(outSize)))
+            return
+        out = torch.empty(int(outSize), dtype=torch.uint8, pin_memory=True)
+        self._bind()
+        check(lib.rsgpu_join(self._h, ctypes.c_void_p(out.data_ptr()), L.ptr_array([_ptr(s) for s in data]),
+                             size, int(outSize)))
+        dst.write(out.numpy().tobytes())
 
     def Verify(self, shards):
         size, dev = self._prep(shards, nilok=False)
