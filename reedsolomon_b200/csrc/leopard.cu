@@ -38,6 +38,7 @@ struct LeoState {
     int device = -1;
     uint16_t *skew16 = nullptr;  // fftSkew, 65535 entries
     uint16_t *t16 = nullptr;     // [65536][kT16Stride] split product tables (see F16)
+    uint16_t *ts16 = nullptr;    // [65535][4][16] nibble tables in fftSkew order (see F16S)
     uint16_t *skew8 = nullptr;   // fftSkew8, 255 entries (widened)
     uint8_t *t8 = nullptr;       // [256][2][16] nibble products
     uint16_t *fold16 = nullptr;  // W_n of FWHT(log) for n = 2^0..2^11 (see leo_errloc_kernel)
@@ -46,6 +47,7 @@ struct LeoState {
         if (device >= 0) {
             cudaFree(skew16);
             cudaFree(t16);
+            cudaFree(ts16);
             cudaFree(skew8);
             cudaFree(t8);
             cudaFree(fold16);
@@ -64,12 +66,14 @@ struct LeoEncArgs {
     long long size;
     const uint16_t *skew;
     const uint16_t *t16;
+    const uint16_t *ts16;
     const uint8_t *t8;
 };
 
 struct LeoDecArgs {
     const uint8_t *shard[kLeoMaxShards];
     const uint16_t *errloc;               // the first n error locators (device)
+    const uint16_t *ts16;
     uint32_t present[kLeoMaxShards / 32];
     uint32_t write[kLeoMaxShards / 32];   // missing shards to reveal
     int k, p, m, n, input_count;
@@ -134,6 +138,14 @@ struct F16 {
     // the slot base has a zero low byte, and the low byte is 2 * index
     // (+128 for the middle part), prepared for four symbols at once.
     const uint16_t *t;
+    const uint16_t *skew;
+    // Butterfly multiplier by fftSkew index: the log value; the modulus
+    // stands for a zero product and skips the multiply (galois_noasm.go:94-112).
+    using C = uint32_t;
+    __device__ __forceinline__ C coef(int idx) const { return skew[idx]; }
+    __device__ __forceinline__ void mac(Q &x, Q y, C lm) const {
+        if (lm != kMod) xor_into(x, mul(y, lm));
+    }
     __device__ __forceinline__ Q mul(Q v, uint32_t lm) const {
         const char *T = reinterpret_cast<const char *>(t);
         const uint32_t base = lm << 9, base2 = base + 256;
@@ -179,6 +191,12 @@ struct F8 {
     // hi nibble 16].  A lookup address is one PRMT of the prepared index
     // byte ((lm & 7) * 32 + 16 * high + nibble) into the 256-byte block of lm.
     uint32_t t;  // shared-space address
+    const uint16_t *skew;
+    using C = uint32_t;
+    __device__ __forceinline__ C coef(int idx) const { return skew[idx]; }
+    __device__ __forceinline__ void mac(Q &x, Q y, C lm) const {
+        if (lm != kMod) xor_into(x, mul(y, lm));
+    }
     __device__ __forceinline__ Q mul(Q v, uint32_t lm) const {
         const uint32_t blk = t + ((lm >> 3) << 8);
         const uint32_t slot = (lm & 7u) * 0x20202020u;
@@ -189,33 +207,112 @@ struct F8 {
         for (int i = 0; i < 4; i++) {
             const uint32_t sel = 0x7650u | (uint32_t)i;
             uint32_t x, y;
-            asm volatile("ld.shared.u8 %0, [%1];" : "=r"(x) : "r"(__byte_perm(lo, blk, sel)));
-            asm volatile("ld.shared.u8 %0, [%1];" : "=r"(y) : "r"(__byte_perm(hi, blk, sel)));
+            asm("ld.shared.u8 %0, [%1];" : "=r"(x) : "r"(__byte_perm(lo, blk, sel)));
+            asm("ld.shared.u8 %0, [%1];" : "=r"(y) : "r"(__byte_perm(hi, blk, sel)));
             r[i] = x ^ y;
         }
         return __byte_perm(__byte_perm(r[0], r[1], 0x0040), __byte_perm(r[2], r[3], 0x0040), 0x5410);
     }
 };
 
+// The table reads below are plain (non-volatile) inline-asm shared loads:
+// their addresses derive from row data loaded after the barrier that ends
+// staging, and their results feed row stores issued before the next barrier,
+// so the compiler can schedule them freely but never across a barrier.
+//
+// GF(2^16) with the transform's multiplier tables staged in shared memory.
+// A transform over fftSkew indices [lo, lo + count) stages, for slot
+// s = index - lo, the four 16-entry nibble product tables of skew[index]
+// (all zero when skew[index] is the modulus, which the reference treats as a
+// zero product, so no test is needed).  Slot s lives in the 256-byte block
+// s >> 1 at half (s & 1) * 128, and its nibble table q at 32-byte position
+// (q + (s >> 2)) & 3 of that half: the four groups a warp covers in the first
+// layer hit different banks.  A lookup address is one PRMT of a prepared
+// index byte into the block base.
+struct F16S : F16 {
+    uint32_t tab;   // shared-space address of slot 0 (256-byte aligned)
+    uint32_t ctab;  // shared-space address of the per-slot index-byte constants (16 B per slot)
+    int lo;         // fftSkew index of slot 0
+    using C = uint32_t;
+    __device__ __forceinline__ C coef(int idx) const { return (uint32_t)(idx - lo); }
+    static __device__ __forceinline__ uint32_t lds16(uint32_t addr) {
+        uint32_t v;
+        asm("ld.shared.u16 %0, [%1];" : "=r"(v) : "r"(addr));
+        return v;
+    }
+    // The position byte of nibble table q of slot s, replicated four times,
+    // is precomputed at staging (slot_consts) and read with one LDS.128.
+    // sw: the slot's bank swizzle (its butterfly group), chosen by the stager
+    static __device__ __forceinline__ uint32_t slot_const(uint32_t s, uint32_t q, uint32_t sw) {
+        return (((s & 1u) << 7) | (((q + sw) & 3u) << 5)) * 0x01010101u;
+    }
+    __device__ __forceinline__ void mac(Q &x, Q y, C s) const {
+        const uint32_t base = tab + ((s >> 1) << 8);
+        uint32_t o0, o1, o2, o3;
+        asm("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
+                     : "=r"(o0), "=r"(o1), "=r"(o2), "=r"(o3) : "r"(ctab + (s << 4)));
+        const uint32_t n0 = ((y.x << 1) & 0x1E1E1E1Eu) | o0;  // 2 * symbol bits 0-3
+        const uint32_t n1 = ((y.x >> 3) & 0x1E1E1E1Eu) | o1;  // bits 4-7
+        const uint32_t n2 = ((y.y << 1) & 0x1E1E1E1Eu) | o2;  // bits 8-11
+        const uint32_t n3 = ((y.y >> 3) & 0x1E1E1E1Eu) | o3;  // bits 12-15
+        uint32_t r[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const uint32_t sel = 0x7650u | (uint32_t)i;
+            r[i] = lds16(__byte_perm(n0, base, sel)) ^ lds16(__byte_perm(n1, base, sel)) ^
+                   lds16(__byte_perm(n2, base, sel)) ^ lds16(__byte_perm(n3, base, sel));
+        }
+        const uint32_t r01 = __byte_perm(r[0], r[1], 0x5410), r23 = __byte_perm(r[2], r[3], 0x5410);
+        x.x ^= __byte_perm(r01, r23, 0x6420);
+        x.y ^= __byte_perm(r01, r23, 0x7531);
+    }
+};
+
+// Copies the nibble tables of fftSkew indices [lo, lo + count) from the
+// skew-ordered global table ([65535][4][16] u16) into the F16S layout, and
+// writes each slot's index-byte constants to ctab.
+// index_of(s): the fftSkew index staged in slot s; swizzle_of(s): its bank
+// swizzle, which must differ between the (up to four) butterfly groups one
+// warp covers in a layer with distance 1.
+template <class IndexOf, class SwizzleOf>
+__device__ void stage_slots(uint8_t *tab, uint4 *ctab, const uint16_t *ts16, unsigned count, IndexOf index_of,
+                            SwizzleOf swizzle_of) {
+    for (unsigned v = threadIdx.x; v < count * 8; v += blockDim.x) {
+        const unsigned s = v >> 3, q = (v >> 1) & 3, h = v & 1;
+        const uint4 x = __ldg(reinterpret_cast<const uint4 *>(ts16 + (size_t)index_of(s) * 64 + q * 16) + h);
+        *reinterpret_cast<uint4 *>(tab + (s >> 1) * 256 + (s & 1) * 128 + ((q + swizzle_of(s)) & 3) * 32 + h * 16) = x;
+    }
+    for (unsigned s = threadIdx.x; s < count; s += blockDim.x) {
+        const unsigned sw = swizzle_of(s);
+        ctab[s] = make_uint4(F16S::slot_const(s, 0, sw), F16S::slot_const(s, 1, sw), F16S::slot_const(s, 2, sw),
+                             F16S::slot_const(s, 3, sw));
+    }
+}
+
+// Contiguous fftSkew indices: slot s = index - lo; group of slot s is s >> 2.
+__device__ void stage_skew_tables(uint8_t *tab, uint4 *ctab, const uint16_t *ts16, int lo, int count) {
+    stage_slots(tab, ctab, ts16, (unsigned)count, [lo](unsigned s) { return (unsigned)lo + s; },
+                [](unsigned s) { return s >> 2; });
+}
+
 // Butterflies (galois_noasm.go:94-112; a log multiplier equal to the modulus
 // stands for multiplication by zero and reduces the butterfly to an XOR).
 template <class F>
-__device__ __forceinline__ void fft2(const F &f, typename F::Q &x, typename F::Q &y, uint32_t lm) {
-    if (lm != F::kMod) F::xor_into(x, f.mul(y, lm));
+__device__ __forceinline__ void fft2(const F &f, typename F::Q &x, typename F::Q &y, typename F::C c) {
+    f.mac(x, y, c);
     F::xor_into(y, x);
 }
 template <class F>
-__device__ __forceinline__ void ifft2(const F &f, typename F::Q &x, typename F::Q &y, uint32_t lm) {
+__device__ __forceinline__ void ifft2(const F &f, typename F::Q &x, typename F::Q &y, typename F::C c) {
     F::xor_into(y, x);
-    if (lm != F::kMod) F::xor_into(x, f.mul(y, lm));
+    f.mac(x, y, c);
 }
 
 // IFFT with decimation in time (ifftDITEncoder leopard.go:764-873 with
 // skew_off = m-1+block*m, ifftDITDecoder :650-693 with skew_off = -1): the
 // layer multipliers are skew[skew_off + iend], [+dist], [+2*dist].
 template <class F>
-__device__ void ifft_rows(const F &f, uint8_t *w, unsigned mtrunc, unsigned m, const uint16_t *skew,
-                          int skew_off) {
+__device__ void ifft_rows(const F &f, uint8_t *w, unsigned mtrunc, unsigned m, int skew_off) {
     using Q = typename F::Q;
     unsigned dist = 1, dist4 = 4, ld = 0;  // dist == 1 << ld
     for (; dist4 <= m; dist = dist4, dist4 <<= 2, ld += 2) {
@@ -224,9 +321,9 @@ __device__ void ifft_rows(const F &f, uint8_t *w, unsigned mtrunc, unsigned m, c
         for (unsigned it = threadIdx.x; it < items; it += blockDim.x) {
             const unsigned q = it >> F::kQuadShift, c = it & (F::kQuads - 1);
             const unsigned r = (q >> ld) << (ld + 2), i = r + (q & (dist - 1)), iend = r + dist;
-            const uint32_t m01 = skew[skew_off + (int)iend];
-            const uint32_t m02 = skew[skew_off + (int)(iend + dist)];
-            const uint32_t m23 = skew[skew_off + (int)(iend + 2 * dist)];
+            const typename F::C m01 = f.coef(skew_off + (int)iend);
+            const typename F::C m02 = f.coef(skew_off + (int)(iend + dist));
+            const typename F::C m23 = f.coef(skew_off + (int)(iend + 2 * dist));
             uint8_t *p0 = w + (size_t)i * kLeoTile;
             uint8_t *p1 = p0 + (size_t)dist * kLeoTile, *p2 = p1 + (size_t)dist * kLeoTile,
                     *p3 = p2 + (size_t)dist * kLeoTile;
@@ -243,7 +340,7 @@ __device__ void ifft_rows(const F &f, uint8_t *w, unsigned mtrunc, unsigned m, c
         __syncthreads();
     }
     if (dist < m) {  // one radix-2 layer left (dist == m / 2)
-        const uint32_t lm = skew[skew_off + (int)dist];
+        const typename F::C lm = f.coef(skew_off + (int)dist);
         const unsigned items = dist << F::kQuadShift;
         for (unsigned it = threadIdx.x; it < items; it += blockDim.x) {
             const unsigned i = it >> F::kQuadShift, c = it & (F::kQuads - 1);
@@ -260,7 +357,7 @@ __device__ void ifft_rows(const F &f, uint8_t *w, unsigned mtrunc, unsigned m, c
 // FFT with decimation in time (fftDIT leopard.go:696-736): multipliers
 // skew[iend-1], [iend+dist-1], [iend+2*dist-1]; groups start below mtrunc.
 template <class F>
-__device__ void fft_rows(const F &f, uint8_t *w, unsigned mtrunc, unsigned m, const uint16_t *skew) {
+__device__ void fft_rows(const F &f, uint8_t *w, unsigned mtrunc, unsigned m) {
     using Q = typename F::Q;
     unsigned dist4 = m, dist = m >> 2;
     unsigned ld = 0;  // dist == 1 << ld
@@ -271,7 +368,8 @@ __device__ void fft_rows(const F &f, uint8_t *w, unsigned mtrunc, unsigned m, co
         for (unsigned it = threadIdx.x; it < items; it += blockDim.x) {
             const unsigned q = it >> F::kQuadShift, c = it & (F::kQuads - 1);
             const unsigned r = (q >> ld) << (ld + 2), i = r + (q & (dist - 1)), iend = r + dist;
-            const uint32_t m01 = skew[iend - 1], m02 = skew[iend + dist - 1], m23 = skew[iend + 2 * dist - 1];
+            const typename F::C m01 = f.coef((int)iend - 1), m02 = f.coef((int)(iend + dist) - 1),
+                                m23 = f.coef((int)(iend + 2 * dist) - 1);
             uint8_t *p0 = w + (size_t)i * kLeoTile;
             uint8_t *p1 = p0 + (size_t)dist * kLeoTile, *p2 = p1 + (size_t)dist * kLeoTile,
                     *p3 = p2 + (size_t)dist * kLeoTile;
@@ -291,7 +389,7 @@ __device__ void fft_rows(const F &f, uint8_t *w, unsigned mtrunc, unsigned m, co
         const unsigned items = ((mtrunc + 1) / 2) << F::kQuadShift;
         for (unsigned it = threadIdx.x; it < items; it += blockDim.x) {
             const unsigned r = 2 * (it >> F::kQuadShift), c = it & (F::kQuads - 1);
-            const uint32_t lm = skew[r];
+            const typename F::C lm = f.coef((int)r);
             uint8_t *p0 = w + (size_t)r * kLeoTile, *p1 = p0 + kLeoTile;
             Q x = F::ld(p0, c), y = F::ld(p1, c);
             fft2(f, x, y, lm);
@@ -326,12 +424,20 @@ __device__ void load_tables8(uint8_t *dst, const uint8_t *src) {
 }
 
 template <class F>
-__device__ __forceinline__ F make_field(const uint16_t *t16, uint8_t *t8_shared);
+__device__ __forceinline__ F make_field(const uint16_t *t16, uint8_t *t8_shared, const uint16_t *skew);
 template <>
-__device__ __forceinline__ F16 make_field<F16>(const uint16_t *t16, uint8_t *) { return F16{t16}; }
+__device__ __forceinline__ F16 make_field<F16>(const uint16_t *t16, uint8_t *, const uint16_t *skew) {
+    F16 f;
+    f.t = t16;
+    f.skew = skew;
+    return f;
+}
 template <>
-__device__ __forceinline__ F8 make_field<F8>(const uint16_t *, uint8_t *t8s) {
-    return F8{(uint32_t)__cvta_generic_to_shared(t8s)};
+__device__ __forceinline__ F8 make_field<F8>(const uint16_t *, uint8_t *t8s, const uint16_t *skew) {
+    F8 f;
+    f.t = (uint32_t)__cvta_generic_to_shared(t8s);
+    f.skew = skew;
+    return f;
 }
 
 constexpr int kT8Bytes = 256 * 32;
@@ -353,18 +459,18 @@ __global__ void __launch_bounds__(kLeoThreads) leo_encode_kernel(const __grid_co
     const unsigned m = (unsigned)a.m;
     uint8_t *tmp = acc + (size_t)m * kLeoTile;
     if (gf8) load_tables8<F>(t8, a.t8);
-    const F f = make_field<F>(a.t16, t8);
+    const F f = make_field<F>(a.t16, t8, a.skew);
     const long long off = (long long)blockIdx.x * kLeoTile;
     const int cnt0 = a.k < (int)m ? a.k : (int)m;
     load_rows<F>(acc, a.shard, 0, cnt0, (int)m, off);
     __syncthreads();
-    ifft_rows(f, acc, (unsigned)cnt0, m, a.skew, (int)m - 1);
+    ifft_rows(f, acc, (unsigned)cnt0, m, (int)m - 1);
     for (int b = 1; b * (int)m < a.k; b++) {
         const int start = b * (int)m;
         const int cnt = a.k - start < (int)m ? a.k - start : (int)m;
         load_rows<F>(tmp, a.shard, start, cnt, (int)m, off);
         __syncthreads();
-        ifft_rows(f, tmp, (unsigned)cnt, m, a.skew, (int)m - 1 + b * (int)m);
+        ifft_rows(f, tmp, (unsigned)cnt, m, (int)m - 1 + b * (int)m);
         for (int v = threadIdx.x; v < (int)m * 4; v += blockDim.x)
             reinterpret_cast<uint4 *>(acc)[v] = make_uint4(
                 reinterpret_cast<uint4 *>(acc)[v].x ^ reinterpret_cast<uint4 *>(tmp)[v].x,
@@ -373,11 +479,204 @@ __global__ void __launch_bounds__(kLeoThreads) leo_encode_kernel(const __grid_co
                 reinterpret_cast<uint4 *>(acc)[v].w ^ reinterpret_cast<uint4 *>(tmp)[v].w);
         __syncthreads();
     }
-    fft_rows(f, acc, (unsigned)a.p, m, a.skew);
+    fft_rows(f, acc, (unsigned)a.p, m);
     for (int v = threadIdx.x; v < a.p * F::kRowParts; v += blockDim.x) {
         const int r = v / F::kRowParts, c = v % F::kRowParts;
         F::row_out(const_cast<uint8_t *>(a.shard[a.k + r]) + off, acc + (size_t)r * kLeoTile, c);
     }
+}
+
+// GF(2^16) encode with each transform's multiplier tables staged in shared
+// memory (F16S): 2m data rows plus (m-1) 128-byte table slots, used while
+// that fits one CTA (m <= 512).
+__global__ void __launch_bounds__(kLeoThreads) leo_encode16_staged_kernel(const __grid_constant__ LeoEncArgs a) {
+    extern __shared__ __align__(16) uint8_t sm[];
+    const unsigned m = (unsigned)a.m;
+    uint8_t *acc = sm, *tmp = sm + (size_t)m * kLeoTile;
+    uint8_t *tab = align_shared256(tmp + (size_t)m * kLeoTile);
+    uint4 *ctab = reinterpret_cast<uint4 *>(tab + (size_t)(m / 2) * 256);
+    F16S f;
+    f.t = a.t16;
+    f.skew = a.skew;
+    f.tab = (uint32_t)__cvta_generic_to_shared(tab);
+    f.ctab = (uint32_t)__cvta_generic_to_shared(ctab);
+    const long long off = (long long)blockIdx.x * kLeoTile;
+    const int cnt0 = a.k < (int)m ? a.k : (int)m;
+    load_rows<F16>(acc, a.shard, 0, cnt0, (int)m, off);
+    f.lo = (int)m;  // block 0 reads fftSkew[m .. 2m-2]
+    stage_skew_tables(tab, ctab, a.ts16, f.lo, (int)m - 1);
+    __syncthreads();
+    ifft_rows(f, acc, (unsigned)cnt0, m, (int)m - 1);
+    for (int b = 1; b * (int)m < a.k; b++) {
+        const int start = b * (int)m;
+        const int cnt = a.k - start < (int)m ? a.k - start : (int)m;
+        load_rows<F16>(tmp, a.shard, start, cnt, (int)m, off);
+        f.lo = (int)m + b * (int)m;
+        stage_skew_tables(tab, ctab, a.ts16, f.lo, (int)m - 1);
+        __syncthreads();
+        ifft_rows(f, tmp, (unsigned)cnt, m, (int)m - 1 + b * (int)m);
+        for (int v = threadIdx.x; v < (int)m * 4; v += blockDim.x) {
+            uint4 x = reinterpret_cast<uint4 *>(acc)[v];
+            const uint4 y = reinterpret_cast<const uint4 *>(tmp)[v];
+            x.x ^= y.x;
+            x.y ^= y.y;
+            x.z ^= y.z;
+            x.w ^= y.w;
+            reinterpret_cast<uint4 *>(acc)[v] = x;
+        }
+        __syncthreads();
+    }
+    f.lo = 0;  // the FFT reads fftSkew[0 .. m-2]
+    stage_skew_tables(tab, ctab, a.ts16, 0, (int)m - 1);
+    __syncthreads();
+    fft_rows(f, acc, (unsigned)a.p, m);
+    for (int v = threadIdx.x; v < a.p * F16::kRowParts; v += blockDim.x) {
+        const int r = v / F16::kRowParts, c = v % F16::kRowParts;
+        F16::row_out(const_cast<uint8_t *>(a.shard[a.k + r]) + off, acc + (size_t)r * kLeoTile, c);
+    }
+}
+
+// ---- GF(2^16) decode with staged tables ---------------------------------
+// The decode transforms span n <= 2048 rows, whose n-1 multipliers do not fit
+// next to the 128 KB of rows, so each layer is staged in chunks of groups:
+// slot 3*(g - g0) + t holds fftSkew[4*dist*g + (t+1)*dist - 1], the t-th
+// multiplier (m01, m02, m23) of group g (ifftDITDecoder / fftDIT index them
+// identically, leopard.go:650-736).
+__device__ void formal_derivative(uint8_t *w, unsigned n);
+
+constexpr unsigned kDecChunkSlots = 672;
+constexpr size_t kDecTableBytes = (size_t)kDecChunkSlots / 2 * 256 + (size_t)kDecChunkSlots * 16;
+
+template <bool kFft>
+__device__ void radix4_staged(const F16S &f, uint8_t *w, uint8_t *tab, uint4 *ctab, const uint16_t *ts16,
+                              unsigned mtrunc, unsigned dist, unsigned ld) {
+    using Q = F16::Q;
+    const unsigned groups = (mtrunc + (dist << 2) - 1) >> (ld + 2);
+    constexpr unsigned kPer = kDecChunkSlots / 3;
+    for (unsigned g0 = 0; g0 < groups; g0 += kPer) {
+        const unsigned cnt = groups - g0 < kPer ? groups - g0 : kPer;
+        stage_slots(tab, ctab, ts16, cnt * 3,
+                    [=](unsigned s) { return 4 * dist * (g0 + s / 3) + (s % 3 + 1) * dist - 1; },
+                    [](unsigned s) { return s / 3; });
+        __syncthreads();
+        const unsigned items = (cnt << ld) << F16::kQuadShift;
+        for (unsigned it = threadIdx.x; it < items; it += blockDim.x) {
+            const unsigned q = it >> F16::kQuadShift, c = it & (F16::kQuads - 1);
+            const unsigned gl = q >> ld;
+            const unsigned r = (g0 + gl) << (ld + 2), i = r + (q & (dist - 1));
+            const uint32_t s01 = gl * 3, s02 = s01 + 1, s23 = s01 + 2;
+            uint8_t *p0 = w + (size_t)i * kLeoTile;
+            uint8_t *p1 = p0 + (size_t)dist * kLeoTile, *p2 = p1 + (size_t)dist * kLeoTile,
+                    *p3 = p2 + (size_t)dist * kLeoTile;
+            Q x0 = F16::ld(p0, c), x1 = F16::ld(p1, c), x2 = F16::ld(p2, c), x3 = F16::ld(p3, c);
+            if (kFft) {
+                fft2(f, x0, x2, s02);
+                fft2(f, x1, x3, s02);
+                fft2(f, x0, x1, s01);
+                fft2(f, x2, x3, s23);
+            } else {
+                ifft2(f, x0, x1, s01);
+                ifft2(f, x2, x3, s23);
+                ifft2(f, x0, x2, s02);
+                ifft2(f, x1, x3, s02);
+            }
+            F16::st(p0, c, x0);
+            F16::st(p1, c, x1);
+            F16::st(p2, c, x2);
+            F16::st(p3, c, x3);
+        }
+        __syncthreads();
+    }
+}
+
+// ifftDITDecoder (leopard.go:650-693) over n rows, groups below mtrunc.
+__device__ void ifft_staged(const F16S &f, uint8_t *w, uint8_t *tab, uint4 *ctab, const uint16_t *ts16,
+                            unsigned mtrunc, unsigned n) {
+    unsigned dist = 1, dist4 = 4, ld = 0;
+    for (; dist4 <= n; dist = dist4, dist4 <<= 2, ld += 2) radix4_staged<false>(f, w, tab, ctab, ts16, mtrunc, dist, ld);
+    if (dist < n) {  // one radix-2 layer left (dist == n / 2): multiplier fftSkew[dist - 1]
+        stage_slots(tab, ctab, ts16, 1, [=](unsigned) { return dist - 1; }, [](unsigned) { return 0u; });
+        __syncthreads();
+        for (unsigned it = threadIdx.x; it < (dist << F16::kQuadShift); it += blockDim.x) {
+            const unsigned i = it >> F16::kQuadShift, c = it & (F16::kQuads - 1);
+            uint8_t *p0 = w + (size_t)i * kLeoTile, *p1 = p0 + (size_t)dist * kLeoTile;
+            F16::Q x = F16::ld(p0, c), y = F16::ld(p1, c);
+            ifft2(f, x, y, 0u);
+            F16::st(p0, c, x);
+            F16::st(p1, c, y);
+        }
+        __syncthreads();
+    }
+}
+
+// fftDIT (leopard.go:696-736) over n rows, groups below mtrunc.
+__device__ void fft_staged(const F16S &f, uint8_t *w, uint8_t *tab, uint4 *ctab, const uint16_t *ts16,
+                           unsigned mtrunc, unsigned n) {
+    unsigned dist4 = n, dist = n >> 2, ld = 0;
+    while ((2u << ld) <= dist) ld++;
+    for (; dist != 0; dist4 = dist, dist >>= 2, ld -= 2) radix4_staged<true>(f, w, tab, ctab, ts16, mtrunc, dist, ld);
+    if (dist4 == 2) {  // final radix-2 layer: pair (r, r+1) multiplied by fftSkew[r]
+        const unsigned pairs = (mtrunc + 1) / 2;
+        for (unsigned p0 = 0; p0 < pairs; p0 += kDecChunkSlots) {
+            const unsigned cnt = pairs - p0 < kDecChunkSlots ? pairs - p0 : kDecChunkSlots;
+            stage_slots(tab, ctab, ts16, cnt, [=](unsigned s) { return 2 * (p0 + s); }, [](unsigned s) { return s; });
+            __syncthreads();
+            for (unsigned it = threadIdx.x; it < (cnt << F16::kQuadShift); it += blockDim.x) {
+                const unsigned sl = it >> F16::kQuadShift, c = it & (F16::kQuads - 1);
+                uint8_t *q0 = w + (size_t)(2 * (p0 + sl)) * kLeoTile, *q1 = q0 + kLeoTile;
+                F16::Q x = F16::ld(q0, c), y = F16::ld(q1, c);
+                fft2(f, x, y, sl);
+                F16::st(q0, c, x);
+                F16::st(q1, c, y);
+            }
+            __syncthreads();
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kLeoDecodeThreads) leo_decode16_staged_kernel(const __grid_constant__ LeoDecArgs a) {
+    extern __shared__ __align__(16) uint8_t sm[];
+    const unsigned n = (unsigned)a.n, m = (unsigned)a.m;
+    uint8_t *w = sm;
+    uint8_t *tab = align_shared256(w + (size_t)n * kLeoTile);
+    uint4 *ctab = reinterpret_cast<uint4 *>(tab + (size_t)kDecChunkSlots / 2 * 256);
+    F16 fg;  // log-indexed tables for the per-row error-locator products
+    fg.t = a.t16;
+    fg.skew = a.skew;
+    F16S fs;
+    fs.t = a.t16;
+    fs.skew = a.skew;
+    fs.tab = (uint32_t)__cvta_generic_to_shared(tab);
+    fs.ctab = (uint32_t)__cvta_generic_to_shared(ctab);
+    fs.lo = 0;
+    const long long off = (long long)blockIdx.x * kLeoTile;
+    for (unsigned it = threadIdx.x; it < (n << F16::kQuadShift); it += blockDim.x) {
+        const unsigned r = it >> F16::kQuadShift, c = it & (F16::kQuads - 1);
+        int src = -1;
+        if (r < (unsigned)a.p) src = a.k + (int)r;
+        else if (r >= m && r < m + (unsigned)a.k) src = (int)(r - m);
+        F16::Q v = F16::zero();
+        if (src >= 0 && bit(a.present, src)) v = fg.mul(F16::ldg(a.shard[src] + off, c), a.errloc[r]);
+        F16::st(w + (size_t)r * kLeoTile, c, v);
+    }
+    __syncthreads();
+    ifft_staged(fs, w, tab, ctab, a.ts16, (unsigned)a.input_count, n);
+    formal_derivative(w, n);
+    fft_staged(fs, w, tab, ctab, a.ts16, m + (unsigned)a.k, n);
+    const unsigned total = (unsigned)(a.k + a.p) << F16::kQuadShift;
+    for (unsigned it = threadIdx.x; it < total; it += blockDim.x) {
+        const int i = (int)(it >> F16::kQuadShift), c = (int)(it & (F16::kQuads - 1));
+        if (!bit(a.write, i)) continue;
+        const unsigned row = i >= a.k ? (unsigned)(i - a.k) : (unsigned)i + m;
+        const uint32_t lm = F16::kMod - a.errloc[row];
+        F16::stg(const_cast<uint8_t *>(a.shard[i]) + off, c, fg.mul(F16::ld(w + (size_t)row * kLeoTile, c), lm));
+    }
+}
+
+// Shared bytes of the staged GF(2^16) encode (0 when it does not fit a CTA).
+size_t staged_encode_smem(unsigned m) {
+    const size_t bytes = (size_t)2 * m * kLeoTile + (size_t)(m / 2) * 256 + (size_t)m * 16 + 256;
+    return bytes <= 227u * 1024u ? bytes : 0;
 }
 
 // Formal derivative (leopard.go:620-623) on n rows in place.  Row x gains
@@ -386,22 +685,27 @@ __global__ void __launch_bounds__(kLeoThreads) leo_encode_kernel(const __grid_co
 // rows are rewritten in ascending chunks with a barrier between the read
 // and write phase of each chunk.
 __device__ void formal_derivative(uint8_t *w, unsigned n) {
-    const unsigned words_per_row = kLeoTile / 4;
-    const unsigned rows_per_chunk = blockDim.x / words_per_row;
-    const unsigned x_local = threadIdx.x / words_per_row, word = threadIdx.x % words_per_row;
+    constexpr unsigned kParts = kLeoTile / 16;  // 16-byte parts per row
+    const unsigned rows_per_chunk = blockDim.x / kParts;
+    const unsigned x_local = threadIdx.x / kParts, part = threadIdx.x % kParts;
+    unsigned lg = 0;
+    while ((2u << lg) <= n) lg++;  // n == 1 << lg
     for (unsigned base = 0; base < n; base += rows_per_chunk) {
         const unsigned x = base + x_local;
-        uint32_t v = 0;
+        uint4 v = make_uint4(0, 0, 0, 0);
         if (x < n) {
-            v = reinterpret_cast<const uint32_t *>(w + (size_t)x * kLeoTile)[word];
-            for (unsigned b = 0; (1u << b) < n; b++) {
-                if ((x >> b) & 1u) continue;
-                const unsigned i = ((x >> b) + 1) << b;
-                if (i < n) v ^= reinterpret_cast<const uint32_t *>(w + (size_t)(x + (1u << b)) * kLeoTile)[word];
+            v = reinterpret_cast<const uint4 *>(w + (size_t)x * kLeoTile)[part];
+            for (unsigned b = 0; b < lg; b++) {
+                if (((x >> b) & 1u) || ((((x >> b) + 1) << b) >= n)) continue;
+                const uint4 y = reinterpret_cast<const uint4 *>(w + (size_t)(x + (1u << b)) * kLeoTile)[part];
+                v.x ^= y.x;
+                v.y ^= y.y;
+                v.z ^= y.z;
+                v.w ^= y.w;
             }
         }
         __syncthreads();
-        if (x < n) reinterpret_cast<uint32_t *>(w + (size_t)x * kLeoTile)[word] = v;
+        if (x < n) reinterpret_cast<uint4 *>(w + (size_t)x * kLeoTile)[part] = v;
         __syncthreads();
     }
 }
@@ -415,7 +719,7 @@ __global__ void __launch_bounds__(kLeoDecodeThreads) leo_decode_kernel(const __g
     uint8_t *w = gf8 ? t8 + kT8Bytes : sm;
     if (gf8) load_tables8<F>(t8, a.t8);
     __syncthreads();
-    const F f = make_field<F>(a.t16, t8);
+    const F f = make_field<F>(a.t16, t8, a.skew);
     const long long off = (long long)blockIdx.x * kLeoTile;
     const unsigned n = (unsigned)a.n, m = (unsigned)a.m;
     // work <- received symbols scaled by their error locators; zeros elsewhere
@@ -430,9 +734,9 @@ __global__ void __launch_bounds__(kLeoDecodeThreads) leo_decode_kernel(const __g
         F::st(w + (size_t)r * kLeoTile, c, v);
     }
     __syncthreads();
-    ifft_rows(f, w, (unsigned)a.input_count, n, a.skew, -1);
+    ifft_rows(f, w, (unsigned)a.input_count, n, -1);
     formal_derivative(w, n);
-    fft_rows(f, w, m + (unsigned)a.k, n, a.skew);
+    fft_rows(f, w, m + (unsigned)a.k, n);
     // reveal: out = work * (modulus - errloc)
     const unsigned total = (unsigned)(a.k + a.p) << F::kQuadShift;
     for (unsigned it = threadIdx.x; it < total; it += blockDim.x) {
@@ -558,6 +862,22 @@ __global__ void build_t16(uint16_t *t, const uint16_t *log, const uint16_t *exp)
     }
 }
 
+// Builds the skew-ordered nibble tables of F16S: entry [i][q][e] =
+// mulLog(e << 4q, fftSkew[i]), zero when fftSkew[i] is the modulus.
+__global__ void build_ts16(uint16_t *t, const uint16_t *skew, const uint16_t *log, const uint16_t *exp) {
+    for (unsigned idx = blockIdx.x * blockDim.x + threadIdx.x; idx < 65535u * 64u; idx += gridDim.x * blockDim.x) {
+        const unsigned i = idx >> 6, q = (idx >> 4) & 3, e = idx & 15;
+        const unsigned lm = skew[i], x = e << (4 * q);
+        uint16_t v = 0;
+        if (x && lm != 65535u) {
+            unsigned s = (unsigned)log[x] + lm;
+            s = (s + (s >> 16)) & 0xFFFF;
+            v = exp[s];
+        }
+        t[idx] = v;
+    }
+}
+
 int ensure_tables(rsgpu_encoder *enc) {
     rsgpu_ctx *ctx = enc->ctx;
     if (enc->leo && enc->leo->device == ctx->device) return RS_OK;
@@ -593,6 +913,9 @@ int ensure_tables(rsgpu_encoder *enc) {
     RS_CUDA(cudaMemcpy(dlog, f16.log.data(), 65536 * 2, cudaMemcpyHostToDevice));
     RS_CUDA(cudaMemcpy(dexp, f16.exp.data(), 65536 * 2, cudaMemcpyHostToDevice));
     build_t16<<<1024, 256, 0, ctx->stream>>>(st->t16, dlog, dexp);
+    RS_CUDA(cudaGetLastError());
+    RS_CUDA(cudaMalloc(&st->ts16, 65535ull * 64 * 2));
+    build_ts16<<<1024, 256, 0, ctx->stream>>>(st->ts16, st->skew16, dlog, dexp);
     RS_CUDA(cudaGetLastError());
     RS_CUDA(cudaStreamSynchronize(ctx->stream));
     cudaFree(dlog);
@@ -660,11 +983,17 @@ int leo_encode_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, size_t size, 
     const bool g16 = is16(enc);
     a.skew = g16 ? enc->leo->skew16 : enc->leo->skew8;
     a.t16 = enc->leo->t16;
+    a.ts16 = enc->leo->ts16;
     a.t8 = enc->leo->t8;
     const size_t smem = (size_t)2 * m * kLeoTile + (g16 ? 0 : kT8Bytes + kT8Slack);
     const int grid = (int)(size / kLeoTile);
     if (!st) st = enc->ctx->stream;
-    if (g16) {
+    const size_t staged = g16 ? staged_encode_smem(m) : 0;
+    if (staged && m >= 4) {
+        rc = set_smem(leo_encode16_staged_kernel, staged);
+        if (rc) return rc;
+        leo_encode16_staged_kernel<<<grid, kLeoThreads, staged, st>>>(a);
+    } else if (g16) {
         rc = set_smem(leo_encode_kernel<F16>, smem);
         if (rc) return rc;
         leo_encode_kernel<F16><<<grid, kLeoThreads, smem, st>>>(a);
@@ -766,12 +1095,13 @@ int leo_reconstruct_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, const ui
     a->size = (long long)size;
     a->skew = g16 ? enc->leo->skew16 : enc->leo->skew8;
     a->t16 = enc->leo->t16;
+    a->ts16 = enc->leo->ts16;
     a->t8 = enc->leo->t8;
-    const size_t smem = (size_t)n * kLeoTile + (g16 ? 0 : kT8Bytes + kT8Slack);
+    const size_t smem = g16 ? (size_t)n * kLeoTile + kDecTableBytes + 256 : (size_t)n * kLeoTile + kT8Bytes + kT8Slack;
     const int grid = (int)(size / kLeoTile);
-    rc = g16 ? set_smem(leo_decode_kernel<F16>, smem) : set_smem(leo_decode_kernel<F8>, smem);
+    rc = g16 ? set_smem(leo_decode16_staged_kernel, smem) : set_smem(leo_decode_kernel<F8>, smem);
     if (rc == RS_OK) {
-        if (g16) leo_decode_kernel<F16><<<grid, kLeoDecodeThreads, smem, st>>>(*a);
+        if (g16) leo_decode16_staged_kernel<<<grid, kLeoDecodeThreads, smem, st>>>(*a);
         else leo_decode_kernel<F8><<<grid, kLeoDecodeThreads, smem, st>>>(*a);
         rc = cuda_status(cudaGetLastError(), "leo_decode_kernel");
     }
