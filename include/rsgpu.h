@@ -45,6 +45,9 @@ extern "C" {
 #define RS_ERR_SINGULAR -10             /* errSingular          matrix.go:184 */
 #define RS_ERR_NOT_SQUARE -11           /* errNotSquare         matrix.go:187 */
 #define RS_ERR_SHORT_DATA -12           /* ErrShortData         reedsolomon.go:1785 */
+#define RS_ERR_RECONSTRUCT_MISMATCH -13 /* ErrReconstructMismatch streaming.go:457 */
+#define RS_ERR_STREAM_READ -14          /* StreamReadError      streaming.go:93-109 */
+#define RS_ERR_STREAM_WRITE -15         /* StreamWriteError     streaming.go:111-127 */
 #define RS_ERR_CUDA -100                /* a CUDA call failed (see rsgpu_last_error) */
 #define RS_ERR_NOMEM -101               /* device or pinned allocation failed */
 #define RS_ERR_TIMEOUT -102             /* a bounded device wait expired */
@@ -246,6 +249,28 @@ int rsgpu_batch_results(rsgpu_batch *batch, int *ok, int n);
 int rsgpu_batch_info(rsgpu_batch *batch, int *n_stripes, int *n_jobs, long long *n_tiles, double *bytes);
 /* Tile size of the persistent launch in bytes (multiple of 4096; 0 = default). */
 int rsgpu_batch_set_tile(rsgpu_batch *batch, int tile_bytes);
+
+/* ---- StreamEncoder (streaming.go:23-700) -----------------------------------
+ * Block-wise Encode / Verify / Reconstruct over caller callbacks (the
+ * reference's io.Reader / io.Writer), classic codec only like rsStream.  A
+ * read callback fills up to `max` bytes of shard `shard` and returns the
+ * count (fewer only at the end of the stream, 0 at its end, < 0 on error); a
+ * write callback returns 0 on success.  Callbacks run on the calling thread
+ * while the device works on the previous block.  `block` is the per-shard
+ * block size (the reference's WithStreamBlockSize, default 4 MiB).  Read and
+ * write failures return RS_ERR_STREAM_READ / RS_ERR_STREAM_WRITE with the
+ * shard index in *err_shard. */
+typedef long long (*rsgpu_read_fn)(void *user, int shard, uint8_t *buf, size_t max);
+typedef int (*rsgpu_write_fn)(void *user, int shard, const uint8_t *buf, size_t n);
+/* Encode (streaming.go:209-245): reads shards 0..k-1, writes k..k+p-1. */
+int rsgpu_stream_encode(rsgpu_encoder *enc, rsgpu_read_fn rd, rsgpu_write_fn wr, void *user, size_t block,
+                        int *err_shard);
+/* Verify (streaming.go:419-444): reads all k+p shards; *ok = 1 when every block verifies. */
+int rsgpu_stream_verify(rsgpu_encoder *enc, rsgpu_read_fn rd, void *user, size_t block, int *ok, int *err_shard);
+/* Reconstruct (streaming.go:453-500): reads shards with valid[i], writes the
+ * rebuilt shards with fill[i]; valid and fill must not both be set. */
+int rsgpu_stream_reconstruct(rsgpu_encoder *enc, const uint8_t *valid, const uint8_t *fill, rsgpu_read_fn rd,
+                             rsgpu_write_fn wr, void *user, size_t block, int *err_shard);
 
 /* ---- request server (no counterpart in the reference) --------------------
  * Continuous batching over device-resident stripes: any host thread submits

@@ -12,6 +12,9 @@ LIB_PATH = os.path.join(_HERE, "librsgpu.so")
 c_u8p = ctypes.POINTER(ctypes.c_uint8)
 c_voidp = ctypes.c_void_p
 c_size = ctypes.c_size_t
+# StreamEncoder callbacks (rsgpu_read_fn / rsgpu_write_fn)
+READ_FN = ctypes.CFUNCTYPE(ctypes.c_longlong, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t)
+WRITE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t)
 c_int = ctypes.c_int
 c_intp = ctypes.POINTER(ctypes.c_int)
 
@@ -108,6 +111,9 @@ SIGNATURES = {
     "rsgpu_split_plan": (c_int, [c_voidp, c_size, c_size, c_voidp, c_voidp]),
     "rsgpu_split": (c_int, [c_voidp, c_voidp, c_size, c_size, c_voidp, c_size, c_voidp, c_voidp]),
     "rsgpu_join": (c_int, [c_voidp, c_voidp, c_voidp, c_size, c_size]),
+    "rsgpu_stream_encode": (c_int, [c_voidp, READ_FN, WRITE_FN, c_voidp, c_size, c_voidp]),
+    "rsgpu_stream_verify": (c_int, [c_voidp, READ_FN, c_voidp, c_size, c_voidp, c_voidp]),
+    "rsgpu_stream_reconstruct": (c_int, [c_voidp, c_voidp, c_voidp, READ_FN, WRITE_FN, c_voidp, c_size, c_voidp]),
     "rsgpu_decode_idx": (c_int, [c_voidp, c_voidp, c_voidp, c_voidp, c_size]),
     "rsgpu_batch_create": (c_int, [c_voidp, c_voidp, ctypes.POINTER(c_voidp)]),
     "rsgpu_batch_destroy": (c_int, [c_voidp]),

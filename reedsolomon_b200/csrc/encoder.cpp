@@ -216,6 +216,9 @@ const char *rsgpu_status_string(int s) {
     case RS_ERR_SINGULAR: return "matrix is singular";
     case RS_ERR_NOT_SQUARE: return "only square matrices can be inverted";
     case RS_ERR_SHORT_DATA: return "not enough data to fill the number of requested shards";
+    case RS_ERR_RECONSTRUCT_MISMATCH: return "valid shards and fill shards are mutually exclusive";
+    case RS_ERR_STREAM_READ: return "error reading stream";
+    case RS_ERR_STREAM_WRITE: return "error writing stream";
     case RS_ERR_CUDA: return "CUDA error";
     case RS_ERR_NOMEM: return "out of device memory";
     case RS_ERR_TIMEOUT: return "device wait timed out";

@@ -42,13 +42,15 @@ ErrReconstructRequired = _err("ErrReconstructRequired", -9)
 ErrSingular = _err("ErrSingular", -10)
 ErrNotSquare = _err("ErrNotSquare", -11)
 ErrShortData = _err("ErrShortData", -12)
+ErrReconstructMismatch = _err("ErrReconstructMismatch", -13)
 CudaError = _err("CudaError", -100)
 ErrNoMem = _err("ErrNoMem", -101)
 ErrTimeout = _err("ErrTimeout", -102)
 ErrNoDevice = _err("ErrNoDevice", -103)
 _BY_CODE = {c.code: c for c in (ErrTooFewShards, ErrShardNoData, ErrShardSize, ErrInvalidShardSize,
                                 ErrInvShardNum, ErrMaxShardNum, ErrNotSupported, ErrInvalidInput,
-                                ErrReconstructRequired, ErrSingular, ErrNotSquare, ErrShortData, CudaError, ErrNoMem,
+                                ErrReconstructRequired, ErrSingular, ErrNotSquare, ErrShortData, ErrReconstructMismatch,
+                                CudaError, ErrNoMem,
                                 ErrTimeout, ErrNoDevice)}
 
 
@@ -114,7 +116,12 @@ def _noop(*_a, **_k):
 WithMaxGoroutines = WithAutoGoroutines = WithMinSplitSize = _noop
 WithSSSE3 = WithAVX2 = WithSSE2 = WithAVX512 = WithGFNI = WithAVXGFNI = _noop
 WithConcurrentStreams = WithConcurrentStreamReads = WithConcurrentStreamWrites = _noop
-WithStreamBlockSize = WithWorkAllocator = _noop
+WithWorkAllocator = _noop
+
+
+def WithStreamBlockSize(n):
+    """Per-shard block size of a StreamEncoder round (options.go:159-167)."""
+    return _opt(stream_block=int(n))
 
 
 # ---- device contexts ----------------------------------------------------------
@@ -169,7 +176,7 @@ class Encoder:
 
     def __init__(self, data_shards, parity_shards, opts):
         o = {"device": 0, "matrix": "default", "fast_one_parity": 0, "leopard": 0,
-             "inversion_cache": 1, "custom": None, "host_only": False}
+             "inversion_cache": 1, "custom": None, "host_only": False, "stream_block": 0}
         for f in opts:
             f(o)
         self._o = o
@@ -524,6 +531,164 @@ class Encoder:
 def New(data_shards, parity_shards, *opts):
     """reedsolomon.New (reedsolomon.go:425)."""
     return Encoder(data_shards, parity_shards, opts)
+
+
+# ---- StreamEncoder (streaming.go) --------------------------------------------
+class StreamReadError(RSError):
+    """A reader failed (streaming.go:93-109); .stream is its shard index."""
+    code = -14
+
+    def __init__(self, err, stream):
+        super().__init__("error reading stream %d: %s" % (stream, err))
+        self.err, self.stream = err, stream
+
+
+class StreamWriteError(RSError):
+    """A writer failed (streaming.go:111-127); .stream is its shard index."""
+    code = -15
+
+    def __init__(self, err, stream):
+        super().__init__("error writing stream %d: %s" % (stream, err))
+        self.err, self.stream = err, stream
+
+
+
+
+class _StreamIO:
+    """ctypes callbacks over Python readers (read/readinto) and writers (write)."""
+
+    def __init__(self, readers, writers):
+        self.readers, self.writers = readers, writers
+        self.exc = None
+        self.read_fn = L.READ_FN(self._read)
+        self.write_fn = L.WRITE_FN(self._write)
+
+    def _read(self, _user, shard, buf, n):
+        try:
+            r = self.readers[shard]
+            view = (ctypes.c_ubyte * n).from_address(buf)
+            if hasattr(r, "readinto"):
+                got = r.readinto(memoryview(view).cast("B"))
+                return int(got or 0)
+            data = r.read(n)
+            ctypes.memmove(buf, data, len(data))
+            return len(data)
+        except Exception as e:  # reported as StreamReadError
+            self.exc = e
+            return -1
+
+    def _write(self, _user, shard, buf, n):
+        try:
+            w = self.writers[shard]
+            m = w.write(ctypes.string_at(buf, n))
+            if m is not None and m != n:
+                raise IOError("short write")
+            return 0
+        except Exception as e:
+            self.exc = e
+            return 1
+
+    def check(self, rc, shard):
+        if rc == -14:
+            raise StreamReadError(self.exc, shard)
+        if rc == -15:
+            raise StreamWriteError(self.exc, shard)
+        check(rc)
+
+
+class StreamEncoder:
+    """StreamEncoder (streaming.go:23-91) over librsgpu: shards are file-like
+    objects, processed in blocks (WithStreamBlockSize, default 4 MiB)."""
+
+    def __init__(self, enc, block):
+        self.enc, self.block = enc, block
+
+    def _run(self, readers, writers, fn):
+        io = _StreamIO(readers, writers)
+        shard = ctypes.c_int(-1)
+        self.enc._bind()
+        rc = fn(io, shard)
+        io.check(rc, shard.value)
+
+    def Encode(self, data, parity):
+        k, p = self.enc.DataShards(), self.enc.ParityShards()
+        if len(data) != k or len(parity) != p:
+            raise ErrTooFewShards("too few shards given")
+        readers = list(data) + [None] * p
+        writers = [None] * k + list(parity)
+        self._run(readers, writers, lambda io, sh: L.lib().rsgpu_stream_encode(
+            self.enc._h, io.read_fn, io.write_fn, None, self.block, ctypes.byref(sh)))
+
+    def Verify(self, shards):
+        if len(shards) != self.enc.TotalShards():
+            raise ErrTooFewShards("too few shards given")
+        ok = ctypes.c_int()
+        self._run(list(shards), [], lambda io, sh: L.lib().rsgpu_stream_verify(
+            self.enc._h, io.read_fn, None, self.block, ctypes.byref(ok), ctypes.byref(sh)))
+        return bool(ok.value)
+
+    def Reconstruct(self, valid, fill):
+        n = self.enc.TotalShards()
+        if len(valid) != n or len(fill) != n:
+            raise ErrTooFewShards("too few shards given")
+        v = L.u8_array([0 if r is None else 1 for r in valid])
+        f = L.u8_array([0 if w is None else 1 for w in fill])
+        self._run(list(valid), list(fill), lambda io, sh: L.lib().rsgpu_stream_reconstruct(
+            self.enc._h, v, f, io.read_fn, io.write_fn, None, self.block, ctypes.byref(sh)))
+
+    def Split(self, data, dst, size):
+        """streaming.go:569-603: `size` bytes of `data` into k writers, zero padded."""
+        if size == 0:
+            raise ErrShortData("not enough data to fill the number of requested shards")
+        k = self.enc.DataShards()
+        if len(dst) != k:
+            raise ErrInvShardNum("cannot create Encoder with less than one data shard or less than zero parity shards")
+        for i, w in enumerate(dst):
+            if w is None:
+                raise StreamWriteError(ErrShardNoData("no shard data"), i)
+        per = (size + k - 1) // k
+        left = size
+        for i in range(k):
+            want = min(per, left)
+            got = b""
+            while len(got) < want:
+                chunk = data.read(want - len(got))
+                if not chunk:
+                    break
+                got += chunk
+            if len(got) != want:
+                raise ErrShortData("not enough data to fill the number of requested shards")
+            left -= want
+            dst[i].write(got + bytes(per - want))
+
+    def Join(self, dst, shards, outSize):
+        """streaming.go:515-553: the first outSize bytes of the data shard readers."""
+        k = self.enc.DataShards()
+        if len(shards) < k:
+            raise ErrTooFewShards("too few shards given")
+        for i in range(k):
+            if shards[i] is None:
+                raise StreamReadError(ErrShardNoData("no shard data"), i)
+        left = outSize
+        for i in range(k):
+            while left:
+                chunk = shards[i].read(min(left, 1 << 20))
+                if not chunk:
+                    break
+                dst.write(chunk)
+                left -= len(chunk)
+        if left:
+            raise ErrShortData("not enough data to fill the number of requested shards")
+
+
+def NewStream(data_shards, parity_shards, *opts):
+    """reedsolomon.NewStream (streaming.go:146-185): at most 256 shards."""
+    if data_shards + parity_shards > 256:
+        raise ErrMaxShardNum("cannot create Encoder with more than 256 data+parity shards")
+    enc = Encoder(data_shards, parity_shards, opts)
+    if enc.codec != RS_CODEC_CLASSIC:
+        raise ErrNotSupported("operation not supported")
+    return StreamEncoder(enc, enc._o["stream_block"] or (4 << 20))
 
 
 def HostOnly():
