@@ -299,6 +299,7 @@ typedef struct rsgpu_completion {
     uint64_t ticket, tag;
     int status;                 /* RS_OK or the request's error */
     double latency_us;          /* submit -> device completion */
+    double queue_us;            /* submit -> launch (admission wait); latency_us - queue_us is service time */
 } rsgpu_completion;
 
 typedef struct rsgpu_server_stats {

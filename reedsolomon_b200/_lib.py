@@ -58,7 +58,7 @@ class RsRequest(ctypes.Structure):
 
 class RsCompletion(ctypes.Structure):
     _fields_ = [("ticket", ctypes.c_uint64), ("tag", ctypes.c_uint64), ("status", c_int),
-                ("latency_us", ctypes.c_double)]
+                ("latency_us", ctypes.c_double), ("queue_us", ctypes.c_double)]
 
 
 class RsServerStats(ctypes.Structure):

@@ -280,16 +280,24 @@ void plan_tiles(rsgpu_batch *b, std::vector<long long> &cta_first) {
     cta_first[grid] = t;
 }
 
-int upload(rsgpu_batch *b) {
+// Uploads the job table and CTA ranges, stream-ordered on `st`: growing a
+// device buffer uses cudaFreeAsync / cudaMallocAsync (doubling), never a
+// device-wide synchronising cudaFree, so a request server can plan one slot's
+// micro-batch while other streams keep running.
+int upload(rsgpu_batch *b, cudaStream_t st) {
     if (!b->dirty) return RS_OK;
     std::vector<long long> cta_first;
     plan_tiles(b, cta_first);
-    auto grow = [](auto *&ptr, size_t &cap, size_t want) -> cudaError_t {
+    auto grow = [st](auto *&ptr, size_t &cap, size_t want) -> cudaError_t {
         if (want <= cap) return cudaSuccess;
-        cudaFree(ptr);
+        want = std::max(want, 2 * cap);
+        if (ptr) {
+            cudaError_t e = cudaFreeAsync(ptr, st);
+            if (e != cudaSuccess) return e;
+        }
         ptr = nullptr;
         cap = 0;
-        cudaError_t e = cudaMalloc((void **)&ptr, want);
+        cudaError_t e = cudaMallocAsync((void **)&ptr, want, st);
         if (e == cudaSuccess) cap = want;
         return e;
     };
@@ -297,8 +305,10 @@ int upload(rsgpu_batch *b) {
     RS_CUDA(grow(b->d_cta, b->d_cta_cap, cta_first.size() * sizeof(long long)));
     RS_CUDA(grow(b->d_flags, b->d_flags_cap, std::max(1, b->n_stripes) * sizeof(int)));
     if (!b->jobs.empty())
-        RS_CUDA(cudaMemcpy(b->d_jobs, b->jobs.data(), b->jobs.size() * sizeof(BatchJob), cudaMemcpyHostToDevice));
-    RS_CUDA(cudaMemcpy(b->d_cta, cta_first.data(), cta_first.size() * sizeof(long long), cudaMemcpyHostToDevice));
+        RS_CUDA(cudaMemcpyAsync(b->d_jobs, b->jobs.data(), b->jobs.size() * sizeof(BatchJob), cudaMemcpyHostToDevice,
+                                st));
+    RS_CUDA(cudaMemcpyAsync(b->d_cta, cta_first.data(), cta_first.size() * sizeof(long long), cudaMemcpyHostToDevice,
+                            st));
     if (b->graph) {
         cudaGraphExecDestroy(b->graph);
         b->graph = nullptr;
@@ -437,7 +447,7 @@ int rsgpu::batch_read_flags(rsgpu_batch *b, int *ok, int n, cudaStream_t st) {
 
 int rsgpu::batch_run_on(rsgpu_batch *b, int mode, cudaStream_t st) {
     rsgpu_ctx *ctx = b->ctx;
-    int rc = upload(b);
+    int rc = upload(b, st);
     if (rc) return rc;
     RS_CUDA(cudaMemsetAsync(b->d_flags, 0, std::max(1, b->n_stripes) * sizeof(int), st));
     if (mode == RS_BATCH_PERSISTENT) {
@@ -498,7 +508,7 @@ int rsgpu_batch_results(rsgpu_batch *b, int *ok, int n) {
 int rsgpu_batch_info(rsgpu_batch *b, int *n_stripes, int *n_jobs, long long *n_tiles, double *bytes) {
     if (!b) return RS_ERR_INVALID_INPUT;
     std::lock_guard<std::recursive_mutex> lk(b->ctx->mu);
-    int rc = upload(b);
+    int rc = upload(b, b->ctx->stream);
     if (rc) return rc;
     if (n_stripes) *n_stripes = b->n_stripes;
     if (n_jobs) *n_jobs = (int)(b->jobs.size() + b->irregular.size());

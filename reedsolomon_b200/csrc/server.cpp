@@ -51,7 +51,7 @@ struct Req {
     size_t footprint = 0;           // algorithmic bytes (reads + writes)
     int status = RS_OK;
     int verify_slot = -1;
-    Clock::time_point t_submit, t_done;
+    Clock::time_point t_submit, t_launch, t_done;
     std::atomic<int64_t> t_kernel_done{0};  // set by a host callback (Leopard stripes)
 };
 
@@ -305,6 +305,8 @@ int admit(rsgpu_server *sv, Slot *s) {
 
 // Plans and launches slot s's requests (caller holds sv->mu).
 void launch(rsgpu_server *sv, Slot *s) {
+    const Clock::time_point now = Clock::now();
+    for (Req *q : s->reqs) q->t_launch = now;
     rsgpu_batch_clear(s->batch);
     bool has_classic = false;
     std::vector<Req *> leo;
@@ -491,6 +493,9 @@ int rsgpu_server_poll(rsgpu_server *sv, rsgpu_completion *out, int max) {
         out[n].tag = q->r.tag;
         out[n].status = q->status;
         out[n].latency_us = std::chrono::duration<double, std::micro>(q->t_done - q->t_submit).count();
+        out[n].queue_us = q->t_launch == Clock::time_point()
+                              ? out[n].latency_us
+                              : std::chrono::duration<double, std::micro>(q->t_launch - q->t_submit).count();
         n++;
     }
     return n;

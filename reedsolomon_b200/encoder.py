@@ -907,6 +907,14 @@ class Server:
             check(n)
         return [(buf[i].ticket, buf[i].tag, buf[i].status, buf[i].latency_us) for i in range(n)]
 
+    def poll_detailed(self, max_n=4096):
+        """Like poll(), with the admission wait: (ticket, tag, status, latency_us, queue_us)."""
+        buf = (L.RsCompletion * max_n)()
+        n = L.lib().rsgpu_server_poll(self._h, buf, max_n)
+        if n < 0:
+            check(n)
+        return [(buf[i].ticket, buf[i].tag, buf[i].status, buf[i].latency_us, buf[i].queue_us) for i in range(n)]
+
     def wait_idle(self, timeout_ms=60000):
         check(L.lib().rsgpu_server_wait_idle(self._h, int(timeout_ms)))
 

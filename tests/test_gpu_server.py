@@ -75,8 +75,9 @@ def test_server_results_alone_equal_mix():
     arrivals = np.cumsum(rng.exponential(50.0, len(reqs)))  # Poisson, 20k req/s offered
     tickets = srv.replay(reqs, arrivals)
     srv.wait_idle(60000)
-    done = srv.poll()
-    assert len(done) == len(reqs) and all(st == 0 for _, _, st, _ in done)
+    done = srv.poll_detailed()
+    assert len(done) == len(reqs) and all(st == 0 for _, _, st, _, _ in done)
+    assert all(0 <= q <= lat for _, _, _, lat, q in done)  # admission wait is part of the latency
     check_results(srv, reqs, expect, tickets)
     st = srv.stats()
     assert st["completed"] == len(reqs) and st["failed"] == 0
