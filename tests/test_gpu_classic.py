@@ -291,6 +291,37 @@ def test_rs10x4_64mib_roundtrip_and_windows():
             assert torch.equal(cp[int(i)], orig[int(i)])
 
 
+def test_shards_past_2gib_offsets():
+    """Shards longer than 2^31 bytes (with a ragged tail for the byte kernel):
+    byte offsets past the 32-bit range must address the right columns in
+    encode, verify and reconstruct (oracle windows across the boundary)."""
+    k, p = 3, 2
+    size = (1 << 31) + 4096 + 48
+    g = torch.Generator(device="cuda").manual_seed(77)
+    sh = [torch.randint(0, 256, (size,), dtype=torch.uint8, device="cuda", generator=g) for _ in range(k)]
+    sh += [torch.empty(size, dtype=torch.uint8, device="cuda") for _ in range(p)]
+    enc = rs.New(k, p)
+    enc.Encode(sh)
+    assert enc.Verify(sh)
+    windows = (0, (1 << 31) - 4096, size - 8192)
+    for off in windows:
+        win = [host(s[off:off + 8192]) for s in sh]
+        want = [w.copy() for w in win]
+        for i in range(k, k + p):
+            want[i][:] = 0
+        O.rs_encode(k, p, want)
+        for i in range(k, k + p):
+            assert np.array_equal(win[i], want[i]), (off, i)
+    keep = {off: [host(s[off:off + 8192]) for s in sh] for off in windows}
+    cp = [None, sh[1], sh[2], None, sh[4]]
+    enc.Reconstruct(cp)
+    for off in windows:
+        assert np.array_equal(host(cp[0][off:off + 8192]), keep[off][0])
+        assert np.array_equal(host(cp[3][off:off + 8192]), keep[off][3])
+    del sh, cp
+    torch.cuda.empty_cache()
+
+
 @pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6])
 def test_every_kernel_variant_bit_exact(variant):
     """Each nibble-address variant of the GF(2^8) kernel gives the oracle's bytes."""

@@ -157,3 +157,35 @@ def test_leopard_rejects_misaligned_shards(gf):
     sh[0] = None
     with pytest.raises(rs.ErrNotSupported):
         enc.Reconstruct(sh)
+
+
+@pytest.mark.parametrize("gf", [16, 8])
+def test_leopard_shards_past_2gib_offsets(gf):
+    """Shards longer than 2^31 bytes: Leopard is local to each 64-byte chunk,
+    so 64-byte aligned windows across the 32-bit boundary must equal the
+    oracle's encode of the same windows, and reconstruct must restore them."""
+    k, p = 4, 2
+    size = (1 << 31) + 128
+    g = torch.Generator(device="cuda").manual_seed(gf)
+    sh = [torch.randint(0, 256, (size,), dtype=torch.uint8, device="cuda", generator=g) for _ in range(k)]
+    sh += [torch.empty(size, dtype=torch.uint8, device="cuda") for _ in range(p)]
+    enc = new(gf, k, p)
+    enc.Encode(sh)
+    windows = (0, (1 << 31) - 4096, size - 4096)
+    keep = {}
+    for off in windows:
+        win = [host(s[off:off + 4096]) for s in sh]
+        want = [w.copy() for w in win]
+        for i in range(k, k + p):
+            want[i][:] = 0
+        O.leo_encode(gf, k, p, want)
+        for i in range(k, k + p):
+            assert np.array_equal(win[i], want[i]), (gf, off, i)
+        keep[off] = win
+    cp = [None, sh[1], sh[2], sh[3], None, sh[5]]
+    enc.Reconstruct(cp)
+    for off in windows:
+        assert np.array_equal(host(cp[0][off:off + 4096]), keep[off][0])
+        assert np.array_equal(host(cp[4][off:off + 4096]), keep[off][4])
+    del sh, cp
+    torch.cuda.empty_cache()
