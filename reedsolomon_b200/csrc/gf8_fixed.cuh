@@ -51,7 +51,16 @@ __global__ void __launch_bounds__(kThreads, MINB) gf8_matmul_fixed(const __grid_
     __syncthreads();
     const uint32_t tab_s = (uint32_t)__cvta_generic_to_shared(tab);
     uint32_t mism = 0;
+    // Verify / xor modes read the outputs too: with one output group those
+    // reads are issued before the multiplies so their latency is hidden.
+    constexpr bool kPrefetchOut = MODE != kModeWrite && G == 1;
     for (; v < nvec; v += stride) {
+        uint4 pre[kPrefetchOut ? 4 : 1];
+        if (kPrefetchOut) {
+#pragma unroll
+            for (int o = 0; o < 4; o++)
+                if (o < a.n_out) pre[o] = __ldcs(reinterpret_cast<const uint4 *>(a.out[o]) + v);
+        }
         uint32_t acc[G][16];
 #pragma unroll
         for (int g = 0; g < G; g++)
@@ -90,11 +99,11 @@ __global__ void __launch_bounds__(kThreads, MINB) gf8_matmul_fixed(const __grid_
                 if (MODE == kModeWrite) {
                     __stcs(dst, w[o]);
                 } else if (MODE == kModeXor) {
-                    uint4 old = __ldcs(dst);
+                    uint4 old = kPrefetchOut ? pre[kPrefetchOut ? o : 0] : __ldcs(dst);
                     old.x ^= w[o].x; old.y ^= w[o].y; old.z ^= w[o].z; old.w ^= w[o].w;
                     __stcs(dst, old);
                 } else {
-                    const uint4 chk = __ldcs(dst);
+                    const uint4 chk = kPrefetchOut ? pre[kPrefetchOut ? o : 0] : __ldcs(dst);
                     mism |= (chk.x ^ w[o].x) | (chk.y ^ w[o].y) | (chk.z ^ w[o].z) | (chk.w ^ w[o].w);
                 }
             }

@@ -265,9 +265,11 @@ int choose_variant(int n_in, int n_out, int mode, size_t nbytes) {
     auto it = g_tuned.find(std::make_tuple(n_in, (n_out + 3) / 4, mode, size_bucket(nbytes)));
     if (it != g_tuned.end()) return it->second;
     // Untuned default: the unrolled kernel with the most resident warps that
-    // does not spill (4 CTAs per SM for up to 4 outputs, 2 for 5-8 outputs);
-    // input counts without a specialisation fall back to kVariantPrmt.
-    return n_out <= 4 ? kVariantFixed4 : kVariantFixed2;
+    // does not spill (up to 4 outputs: 4 CTAs per SM when writing, 3 when the
+    // outputs are also read, which holds them in registers; 2 for 5-8
+    // outputs); input counts without a specialisation fall back to kVariantPrmt.
+    if (n_out > 4) return kVariantFixed2;
+    return mode == kModeWrite ? kVariantFixed4 : kVariantFixed3;
 }
 
 void record_variant(int n_in, int n_out, int mode, size_t nbytes, int v) {
