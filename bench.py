@@ -485,15 +485,20 @@ def extra_serving(dev, n_req=1200, load=0.7, seed=55):
         srv.reset_stats()
         tickets = srv.replay(reqs, arrivals)
         srv.wait_idle(600000)
-        done = srv.poll(len(reqs) + 16)
+        done = srv.poll_detailed(len(reqs) + 16)
         st = srv.stats()
         fails = sum(1 for d in done if d[2] != 0)
         ok &= fails == 0 and len(done) == len(reqs)
         data_bytes = sum(r["k"] * r["size"] for r in reqs)
-        by_op = {}
-        lat = {t: l for t, _, _, l in done}
+        by_op, queue, service = {}, {}, {}
+        lat = {t: (l, q) for t, _, _, l, q in done}
         for r, t in zip(reqs, tickets):
-            by_op.setdefault(r["op"] + ("_leopard" if r["leopard"] else "_classic"), []).append(lat.get(t, 0.0))
+            kind = r["op"] + ("_leopard" if r["leopard"] else "_classic")
+            lq = lat.get(t, (0.0, 0.0))
+            by_op.setdefault(kind, []).append(lq[0])
+            lane = "leopard" if r["leopard"] else "classic"
+            queue.setdefault(lane, []).append(lq[1])
+            service.setdefault(lane, []).append(lq[0] - lq[1])
         # every reconstructed shard equals the original bytes
         scratch = torch.empty(SERVE_MAX, dtype=torch.uint8, device=dev)
         for r, t in zip(reqs, tickets):
@@ -511,7 +516,11 @@ def extra_serving(dev, n_req=1200, load=0.7, seed=55):
                 "latency_us_max": round(st["max_us"], 1), "elapsed_s": round(st["elapsed_s"], 3),
                 "max_inflight_GB": round(st["max_inflight_bytes"] / 1e9, 2),
                 "p50_us_by_kind": {kk: round(_pct(v, 50), 1) for kk, v in sorted(by_op.items())},
-                "p99_us_by_kind": {kk: round(_pct(v, 99), 1) for kk, v in sorted(by_op.items())}}
+                "p99_us_by_kind": {kk: round(_pct(v, 99), 1) for kk, v in sorted(by_op.items())},
+                "admission_wait_us_p50_p99": {kk: [round(_pct(v, 50), 1), round(_pct(v, 99), 1)]
+                                              for kk, v in sorted(queue.items())},
+                "service_us_p50_p99": {kk: [round(_pct(v, 50), 1), round(_pct(v, 99), 1)]
+                                       for kk, v in sorted(service.items())}}
 
     phase([0.0] * 64, seed + 100)  # warm: encoders, tables, error locators of the warm patterns
     burst = phase([0.0] * n_req, seed + 1)
