@@ -281,14 +281,15 @@ void plan_tiles(rsgpu_batch *b, std::vector<long long> &cta_first) {
 }
 
 // Uploads the job table and CTA ranges, stream-ordered on `st`: growing a
-// device buffer uses cudaFreeAsync / cudaMallocAsync (doubling), never a
-// device-wide synchronising cudaFree, so a request server can plan one slot's
-// micro-batch while other streams keep running.
+// device buffer uses cudaFreeAsync and the context's stream-ordered pool
+// (doubling), never a device-wide synchronising cudaFree, so a request
+// server can plan one slot's micro-batch while other streams keep running.
 int upload(rsgpu_batch *b, cudaStream_t st) {
     if (!b->dirty) return RS_OK;
     std::vector<long long> cta_first;
     plan_tiles(b, cta_first);
-    auto grow = [st](auto *&ptr, size_t &cap, size_t want) -> cudaError_t {
+    cudaMemPool_t pool = b->ctx->pool;
+    auto grow = [st, pool](auto *&ptr, size_t &cap, size_t want) -> cudaError_t {
         if (want <= cap) return cudaSuccess;
         want = std::max(want, 2 * cap);
         if (ptr) {
@@ -297,7 +298,7 @@ int upload(rsgpu_batch *b, cudaStream_t st) {
         }
         ptr = nullptr;
         cap = 0;
-        cudaError_t e = cudaMallocAsync((void **)&ptr, want, st);
+        cudaError_t e = cudaMallocFromPoolAsync((void **)&ptr, want, pool, st);
         if (e == cudaSuccess) cap = want;
         return e;
     };

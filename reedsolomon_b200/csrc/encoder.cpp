@@ -248,6 +248,21 @@ int rsgpu_ctx_create(int device, rsgpu_ctx **out) {
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy_out, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&c->d_flag, sizeof(int));
     if (e == cudaSuccess) e = cudaHostAlloc(&c->h_flag, sizeof(int), cudaHostAllocDefault);
+    if (e == cudaSuccess) {
+        // Private stream-ordered pool for small per-call scratch (Leopard error
+        // locators, batch job tables): its memory is kept across
+        // synchronisations, so steady-state calls never map memory.
+        cudaMemPoolProps props;
+        memset(&props, 0, sizeof props);
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        e = cudaMemPoolCreate(&c->pool, &props);
+        if (e == cudaSuccess) {
+            uint64_t keep = ~0ull;
+            e = cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    }
     if (e != cudaSuccess) {
         int rc = cuda_status(e, "rsgpu_ctx_create");
         rsgpu_ctx_destroy(c);
@@ -270,6 +285,7 @@ int rsgpu_ctx_destroy(rsgpu_ctx *c) {
     if (c->copy_in) cudaStreamDestroy(c->copy_in);
     if (c->copy_out) cudaStreamDestroy(c->copy_out);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    if (c->pool) cudaMemPoolDestroy(c->pool);
     delete c;
     return RS_OK;
 }

@@ -1069,7 +1069,7 @@ int leo_reconstruct_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, const ui
     if (!st) st = enc->ctx->stream;
     // error locators on the device: stream-ordered scratch, freed behind the decode
     uint16_t *d_el = nullptr;
-    RS_CUDA(cudaMallocAsync((void **)&d_el, (size_t)n * sizeof(uint16_t), st));
+    RS_CUDA(cudaMallocFromPoolAsync((void **)&d_el, (size_t)n * sizeof(uint16_t), enc->ctx->pool, st));
     LeoErrArgs ea;
     memset(&ea, 0, sizeof ea);
     memcpy(ea.present, a->present, sizeof ea.present);

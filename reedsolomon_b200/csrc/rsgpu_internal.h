@@ -48,6 +48,7 @@ struct rsgpu_ctx {
     rsgpu::DeviceBuffer staging;  // host-path device copies of shards
     std::vector<cudaEvent_t> events;
     std::shared_ptr<rsgpu::LeoState> leo;  // Leopard tables, built on first use
+    cudaMemPool_t pool = nullptr;  // stream-ordered scratch (keeps its memory, never trims)
 };
 
 struct rsgpu_encoder {
