@@ -74,7 +74,7 @@ int read_block(Pipeline &pl, Slot &s, const uint8_t *want, rsgpu_read_fn rd, voi
         size_t got = 0;
         while (got < pl.block) {  // io.ReadFull
             const long long n = rd(user, i, pl.h(s, i) + got, pl.block - got);
-            if (n < 0) {
+            if (n < 0 || n > (long long)(pl.block - got)) {  // an error, or more than was asked for
                 if (err_shard) *err_shard = i;
                 return RS_ERR_STREAM_READ;
             }
