@@ -405,8 +405,18 @@ void worker_loop(rsgpu_server *sv) {
                 progress = true;
             }
         }
-        if (!progress) sv->cv.wait_for(lk, std::chrono::microseconds(20));
-        else sv->cv.notify_all();
+        if (!progress) {
+            bool busy = false;
+            for (Slot *s : sv->slots) busy |= s->busy;
+            // Idle: sleep until a submit or shutdown (both change the state
+            // under the lock before notifying, so no wakeup is lost).  With work on the device, poll
+            // every 20 us as well: completion callbacks notify without the
+            // lock and may race with this check.
+            if (!busy && queues_empty(sv) && !sv->stop) sv->cv.wait(lk);
+            else sv->cv.wait_for(lk, std::chrono::microseconds(20));
+        } else {
+            sv->cv.notify_all();
+        }
     }
     sv->cv.notify_all();
 }
