@@ -479,9 +479,10 @@ def extra_serving(dev, n_req=1200, load=0.7, seed=55):
            "requests": n_req, "mix": "60% encode / 40% reconstruct, 4 KiB-4 MiB log-uniform, erasures U[1,p]"}
     ok = True
 
-    def phase(arrivals, seed_r):
+    def phase(arrivals, seed_r, reqs=None):
         nonlocal ok
-        reqs = serving_requests(pools, n_req, seed_r)
+        if reqs is None:
+            reqs = serving_requests(pools, n_req, seed_r)
         srv.reset_stats()
         tickets = srv.replay(reqs, arrivals)
         srv.wait_idle(600000)
@@ -513,7 +514,7 @@ def extra_serving(dev, n_req=1200, load=0.7, seed=55):
                 "data_GBps": round(data_bytes / st["elapsed_s"] / 1e9, 1) if st["elapsed_s"] else None,
                 "footprint_GBps": round(st["bytes"] / st["elapsed_s"] / 1e9, 1) if st["elapsed_s"] else None,
                 "latency_us_p50": round(st["p50_us"], 1), "latency_us_p99": round(st["p99_us"], 1),
-                "latency_us_max": round(st["max_us"], 1), "elapsed_s": round(st["elapsed_s"], 3),
+                "latency_us_max": round(st["max_us"], 1), "elapsed_s": round(st["elapsed_s"], 6),
                 "max_inflight_GB": round(st["max_inflight_bytes"] / 1e9, 2),
                 "p50_us_by_kind": {kk: round(_pct(v, 50), 1) for kk, v in sorted(by_op.items())},
                 "p99_us_by_kind": {kk: round(_pct(v, 99), 1) for kk, v in sorted(by_op.items())},
@@ -531,6 +532,37 @@ def extra_serving(dev, n_req=1200, load=0.7, seed=55):
     poisson = phase(arrivals, seed + 3)
     poisson["offered_req_per_s"] = round(rate, 1)
     out["poisson"] = poisson
+    # Batching value for small stripes: the classic requests of the burst mix
+    # through the server vs one synchronous C-ABI call per request (what a
+    # server without batching would issue), same stripes and outputs.
+    reqs_c = [r for r in serving_requests(pools, n_req, seed + 1) if not r["leopard"]]
+    served_c = phase([0.0] * len(reqs_c), 0, reqs_c)
+    lib = rs.lib()
+    encs = {(k, p): rs.New(k, p) for k, p, leo in SERVE_GEOS if not leo}
+    outs = {key: [torch.empty(SERVE_MAX, dtype=torch.uint8, device=dev) for _ in range(key[1])] for key in encs}
+    for e in encs.values():
+        e.ctx.bind_current_stream()
+    calls = []
+    for r in reqs_c:
+        e = encs[(r["k"], r["p"])]
+        if r["op"] == "encode":
+            calls.append((True, e, rs._lib.ptr_array([t.data_ptr() for t in r["shards"]]), None, r["size"]))
+        else:
+            spare = iter(outs[(r["k"], r["p"])])
+            ptrs = rs._lib.ptr_array([(t if t is not None else next(spare)).data_ptr() for t in r["shards"]])
+            calls.append((False, e, ptrs, rs._lib.u8_array(r["present"]), r["size"]))
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for is_enc, e, ptrs, pres, size in calls:
+        if is_enc:
+            rs.encoder.check(lib.rsgpu_encode(e._h, ptrs, size))
+        else:
+            rs.encoder.check(lib.rsgpu_reconstruct(e._h, ptrs, pres, size, None))
+    per_call_s = time.perf_counter() - t0
+    out["classic_only"] = {"requests": len(reqs_c), "server_burst_s": served_c["elapsed_s"],
+                           "per_call_sync_s": round(per_call_s, 4),
+                           "speedup_server_vs_per_call": round(per_call_s / served_c["elapsed_s"], 2)
+                           if served_c["elapsed_s"] else None}
     out["outputs_bit_exact"] = bool(ok)
     srv.close()
     del pools
