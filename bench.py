@@ -536,6 +536,7 @@ def extra_serving(dev, n_req=1200, load=0.7, seed=55):
     # through the server vs one synchronous C-ABI call per request (what a
     # server without batching would issue), same stripes and outputs.
     reqs_c = [r for r in serving_requests(pools, n_req, seed + 1) if not r["leopard"]]
+    phase([0.0] * len(reqs_c), 0, reqs_c)  # warm: the classic slots' planners and encoders
     served_c = phase([0.0] * len(reqs_c), 0, reqs_c)
     lib = rs.lib()
     encs = {(k, p): rs.New(k, p) for k, p, leo in SERVE_GEOS if not leo}
@@ -551,6 +552,11 @@ def extra_serving(dev, n_req=1200, load=0.7, seed=55):
             spare = iter(outs[(r["k"], r["p"])])
             ptrs = rs._lib.ptr_array([(t if t is not None else next(spare)).data_ptr() for t in r["shards"]])
             calls.append((False, e, ptrs, rs._lib.u8_array(r["present"]), r["size"]))
+    for is_enc, e, ptrs, pres, size in calls[:64]:  # warm
+        if is_enc:
+            rs.encoder.check(lib.rsgpu_encode(e._h, ptrs, size))
+        else:
+            rs.encoder.check(lib.rsgpu_reconstruct(e._h, ptrs, pres, size, None))
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
     for is_enc, e, ptrs, pres, size in calls:
