@@ -16,6 +16,7 @@
 
 #include "gf8_device.cuh"
 #include "rsgpu_internal.h"
+#include "trace.h"
 
 namespace rsgpu {
 namespace {
@@ -428,6 +429,7 @@ int rsgpu_batch_add(rsgpu_batch *b, const rsgpu_stripe *s, int n) {
 }
 
 int rsgpu_batch_run_async(rsgpu_batch *b, int mode) {
+    RS_TRACE("rsgpu_batch_run_async");
     if (!b) return RS_ERR_INVALID_INPUT;
     std::lock_guard<std::recursive_mutex> lk(b->ctx->mu);
     return batch_run_on(b, mode, b->ctx->stream);

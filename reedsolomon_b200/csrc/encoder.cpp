@@ -10,6 +10,7 @@
 #include <string>
 
 #include "rsgpu_internal.h"
+#include "trace.h"
 
 namespace rsgpu {
 
@@ -425,6 +426,7 @@ int rsgpu_encoder_matrix(const rsgpu_encoder *enc, uint8_t *out) {
     } while (0)
 
 int rsgpu_encode(rsgpu_encoder *enc, uint8_t *const *shards, size_t size) {
+    RS_TRACE("rsgpu_encode");
     NEED_CTX(enc);
     std::lock_guard<std::recursive_mutex> lk(enc->ctx->mu);
     int rc = check_ptrs(shards, enc->total);
@@ -439,6 +441,7 @@ int rsgpu_encode(rsgpu_encoder *enc, uint8_t *const *shards, size_t size) {
 }
 
 int rsgpu_encode_async(rsgpu_encoder *enc, uint8_t *const *shards, size_t size) {
+    RS_TRACE("rsgpu_encode_async");
     NEED_CTX(enc);
     std::lock_guard<std::recursive_mutex> lk(enc->ctx->mu);
     int rc = check_ptrs(shards, enc->total);
@@ -479,6 +482,7 @@ int rsgpu_reconstruct_async(rsgpu_encoder *enc, uint8_t *const *shards, const ui
 
 int rsgpu_encode_idx(rsgpu_encoder *enc, const uint8_t *data, int idx, uint8_t *const *parity,
                      size_t size) {
+    RS_TRACE("rsgpu_encode_idx");
     NEED_CTX(enc);
     if (enc->codec != RS_CODEC_CLASSIC) return RS_ERR_NOT_SUPPORTED;  // leopard.go:272
     std::lock_guard<std::recursive_mutex> lk(enc->ctx->mu);
@@ -538,6 +542,7 @@ int rsgpu_split_plan(rsgpu_encoder *enc, size_t len, size_t cap, size_t *per_sha
 
 int rsgpu_split(rsgpu_encoder *enc, uint8_t *data, size_t len, size_t cap, uint8_t *padding,
                 size_t padding_bytes, uint8_t **shards, size_t *per_shard) {
+    RS_TRACE("rsgpu_split");
     NEED_CTX(enc);
     if (!shards || !per_shard) return RS_ERR_INVALID_INPUT;
     SplitLayout L;
@@ -567,6 +572,7 @@ int rsgpu_split(rsgpu_encoder *enc, uint8_t *data, size_t len, size_t cap, uint8
 }
 
 int rsgpu_join(rsgpu_encoder *enc, void *dst, uint8_t *const *shards, size_t shard_size, size_t out_size) {
+    RS_TRACE("rsgpu_join");
     NEED_CTX(enc);
     if (!shards) return RS_ERR_TOO_FEW_SHARDS;
     size_t have = 0;
@@ -589,6 +595,7 @@ int rsgpu_join(rsgpu_encoder *enc, void *dst, uint8_t *const *shards, size_t sha
 }
 
 int rsgpu_update(rsgpu_encoder *enc, uint8_t *const *shards, const uint8_t *const *new_data, size_t size) {
+    RS_TRACE("rsgpu_update");
     NEED_CTX(enc);
     if (enc->codec != RS_CODEC_CLASSIC) return RS_ERR_NOT_SUPPORTED;  // leopard.go:316, leopard8.go:289
     if (!shards || !new_data) return RS_ERR_TOO_FEW_SHARDS;
@@ -622,6 +629,7 @@ int rsgpu_update(rsgpu_encoder *enc, uint8_t *const *shards, const uint8_t *cons
 
 int rsgpu_decode_idx(rsgpu_encoder *enc, uint8_t *const *dst, const uint8_t *expect,
                      const uint8_t *const *input, size_t size) {
+    RS_TRACE("rsgpu_decode_idx");
     NEED_CTX(enc);
     if (enc->codec != RS_CODEC_CLASSIC) return RS_ERR_NOT_SUPPORTED;  // leopard.go:94, leopard8.go:90
     if (!dst || !input) return RS_ERR_INVALID_INPUT;
@@ -693,6 +701,7 @@ int rsgpu_decode_idx(rsgpu_encoder *enc, uint8_t *const *dst, const uint8_t *exp
 }
 
 int rsgpu_verify(rsgpu_encoder *enc, uint8_t *const *shards, size_t size, int *ok) {
+    RS_TRACE("rsgpu_verify");
     NEED_CTX(enc);
     if (!ok) return RS_ERR_INVALID_INPUT;
     std::lock_guard<std::recursive_mutex> lk(enc->ctx->mu);
@@ -712,6 +721,7 @@ int rsgpu_verify(rsgpu_encoder *enc, uint8_t *const *shards, size_t size, int *o
 static int reconstruct_common(rsgpu_encoder *enc, uint8_t **shards, const uint8_t *present,
                               size_t size, int data_only, const uint8_t *required, int n_required,
                               uint8_t *written) {
+    RS_TRACE(data_only ? "rsgpu_reconstruct_data" : "rsgpu_reconstruct");
     NEED_CTX(enc);
     if (!shards || !present) return RS_ERR_TOO_FEW_SHARDS;
     std::lock_guard<std::recursive_mutex> lk(enc->ctx->mu);
@@ -763,6 +773,7 @@ int rsgpu_decode_plan(rsgpu_encoder *enc, const uint8_t *present, int data_only,
 int rsgpu_code_some_shards(rsgpu_ctx *ctx, const uint8_t *rows, int n_in, int n_out,
                            const uint8_t *const *in, uint8_t *const *out, size_t start, size_t stop,
                            int clear) {
+    RS_TRACE("rsgpu_code_some_shards");
     if (!ctx) return RS_ERR_NO_DEVICE;
     if (!rows || !in || !out || n_in <= 0 || n_out < 0 || stop < start) return RS_ERR_INVALID_INPUT;
     std::lock_guard<std::recursive_mutex> lk(ctx->mu);
@@ -780,6 +791,7 @@ int rsgpu_code_some_shards(rsgpu_ctx *ctx, const uint8_t *rows, int n_in, int n_
 int rsgpu_check_some_shards(rsgpu_ctx *ctx, const uint8_t *rows, int n_in, int n_out,
                             const uint8_t *const *in, const uint8_t *const *to_check, size_t nbytes,
                             int *ok) {
+    RS_TRACE("rsgpu_check_some_shards");
     if (!ctx) return RS_ERR_NO_DEVICE;
     if (!ok || !rows || !in || !to_check || n_in <= 0 || n_out < 0) return RS_ERR_INVALID_INPUT;
     std::lock_guard<std::recursive_mutex> lk(ctx->mu);
@@ -810,6 +822,7 @@ int rsgpu_slice_xor(rsgpu_ctx *ctx, const uint8_t *in, uint8_t *out, size_t n) {
 
 int rsgpu_autotune_gf8(rsgpu_ctx *ctx, int n_in, int n_out, size_t nbytes, int mode, int reps,
                        float *ms_out, int *best_out) {
+    RS_TRACE("rsgpu_autotune_gf8");
     if (!ctx) return RS_ERR_NO_DEVICE;
     if (n_in <= 0 || n_in > kMaxIn || n_out <= 0 || n_out > kMaxOut || nbytes == 0 || mode < 0 ||
         mode > kModeVerify)

@@ -9,6 +9,7 @@
 #include <cstring>
 
 #include "rsgpu_internal.h"
+#include "trace.h"
 
 namespace rsgpu {
 namespace {
@@ -88,6 +89,7 @@ int run_pipeline(rsgpu_ctx *ctx, const std::vector<uint8_t *> &host_rows, const 
 using namespace rsgpu;
 
 extern "C" int rsgpu_encode_host(rsgpu_encoder *enc, uint8_t *const *host, size_t size) {
+    RS_TRACE("rsgpu_encode_host");
     if (!enc) return RS_ERR_INVALID_INPUT;
     if (!enc->ctx) return RS_ERR_NO_DEVICE;
     if (!host) return RS_ERR_TOO_FEW_SHARDS;
@@ -117,6 +119,7 @@ extern "C" int rsgpu_encode_host(rsgpu_encoder *enc, uint8_t *const *host, size_
 
 extern "C" int rsgpu_reconstruct_host(rsgpu_encoder *enc, uint8_t **host, const uint8_t *present,
                                       size_t size, int data_only, uint8_t *written) {
+    RS_TRACE("rsgpu_reconstruct_host");
     if (!enc) return RS_ERR_INVALID_INPUT;
     if (!enc->ctx) return RS_ERR_NO_DEVICE;
     if (!host || !present) return RS_ERR_TOO_FEW_SHARDS;

@@ -31,6 +31,7 @@
 
 #include "leo_host.h"
 #include "rsgpu_internal.h"
+#include "trace.h"
 
 using Clock = std::chrono::steady_clock;
 
@@ -305,6 +306,7 @@ int admit(rsgpu_server *sv, Slot *s) {
 
 // Plans and launches slot s's requests (caller holds sv->mu).
 void launch(rsgpu_server *sv, Slot *s) {
+    RS_TRACE(s->lane ? "rsgpu_server micro-batch (leopard)" : "rsgpu_server micro-batch (classic)");
     const Clock::time_point now = Clock::now();
     for (Req *q : s->reqs) q->t_launch = now;
     rsgpu_batch_clear(s->batch);

@@ -17,6 +17,7 @@
 #include <cstring>
 
 #include "rsgpu_internal.h"
+#include "trace.h"
 
 using namespace rsgpu;
 
@@ -117,6 +118,7 @@ extern "C" {
 
 int rsgpu_stream_encode(rsgpu_encoder *enc, rsgpu_read_fn rd, rsgpu_write_fn wr, void *user, size_t block,
                         int *err_shard) {
+    RS_TRACE("rsgpu_stream_encode");
     if (!enc) return RS_ERR_INVALID_INPUT;
     if (!enc->ctx) return RS_ERR_NO_DEVICE;
     if (!classic_ok(enc)) return RS_ERR_NOT_SUPPORTED;  // rsStream wraps the classic codec
@@ -179,6 +181,7 @@ int rsgpu_stream_encode(rsgpu_encoder *enc, rsgpu_read_fn rd, rsgpu_write_fn wr,
 }
 
 int rsgpu_stream_verify(rsgpu_encoder *enc, rsgpu_read_fn rd, void *user, size_t block, int *ok, int *err_shard) {
+    RS_TRACE("rsgpu_stream_verify");
     if (!enc || !ok) return RS_ERR_INVALID_INPUT;
     if (!enc->ctx) return RS_ERR_NO_DEVICE;
     if (!classic_ok(enc)) return RS_ERR_NOT_SUPPORTED;
@@ -248,6 +251,7 @@ int rsgpu_stream_verify(rsgpu_encoder *enc, rsgpu_read_fn rd, void *user, size_t
 
 int rsgpu_stream_reconstruct(rsgpu_encoder *enc, const uint8_t *valid, const uint8_t *fill, rsgpu_read_fn rd,
                              rsgpu_write_fn wr, void *user, size_t block, int *err_shard) {
+    RS_TRACE("rsgpu_stream_reconstruct");
     if (!enc || !valid || !fill) return RS_ERR_INVALID_INPUT;
     if (!enc->ctx) return RS_ERR_NO_DEVICE;
     if (!classic_ok(enc)) return RS_ERR_NOT_SUPPORTED;
