@@ -339,7 +339,30 @@ int rsgpu_autotune_gf8(rsgpu_ctx *ctx, int n_in, int n_out, size_t nbytes, int m
                        float *ms_out, int *best_out);
 /* Force one variant for every launch (-1 restores the tuned choice). */
 int rsgpu_force_variant(int variant);
+/* Records a tuning result without timing (e.g. one saved from an earlier
+ * rsgpu_autotune_gf8): launches of this geometry, mode and size bucket use
+ * `variant`; -1 removes the record (the untuned default applies again). */
+int rsgpu_record_variant(int n_in, int n_out, size_t nbytes, int mode, int variant);
 int rsgpu_num_variants(void);
+
+/* ---- run-time generated XOR-network kernels (variant 7).  No counterpart
+ * in the reference, whose per-shape kernels are generated at build time
+ * (_gen/gen.go) and whose GFNI path applies the same 8x8 bit matrices
+ * (genGFNIMatrix, galois.go:1004-1016) one coefficient at a time. -------- */
+/* 1 when NVRTC is loadable and variant 7 can run, else 0. */
+int rsgpu_xornet_available(void);
+/* Waits for queued background compiles; returns how many XOR-network
+ * kernels are compiled in this process. */
+int rsgpu_xornet_sync(void);
+/* Generated source for an n_out x n_in coefficient tile (row-major,
+ * n_in <= 32, n_out <= 16) in one mode (0 write, 1 xor into the outputs,
+ * 2 compare with them), factoring `group` inputs at a time (0: the default
+ * for n_out): the CUDA kernel (host == 0) or the same schedule as a plain C
+ * function rs_xornet_host(in, out, nchunk, flag) over host arrays
+ * (host == 1).  Copies at most cap bytes including the NUL and returns the
+ * full length without it, or a negative status. */
+long long rsgpu_xornet_source(const uint8_t *coef, int n_in, int n_out, int mode, int group, int host,
+                              char *buf, size_t cap);
 
 /* ---- host algebra (CPU only, no device needed) --------------------------- */
 /* buildMatrix* (reedsolomon.go:232-413): (total x k) row-major */

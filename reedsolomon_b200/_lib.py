@@ -107,6 +107,11 @@ SIGNATURES = {
     "rsgpu_autotune_gf8": (c_int, [c_voidp, c_int, c_int, c_size, c_int, c_int, c_voidp, c_intp]),
     "rsgpu_force_variant": (c_int, [c_int]),
     "rsgpu_num_variants": (c_int, []),
+    "rsgpu_record_variant": (c_int, [c_int, c_int, c_size, c_int, c_int]),
+    "rsgpu_xornet_available": (c_int, []),
+    "rsgpu_xornet_sync": (c_int, []),
+    "rsgpu_xornet_source": (ctypes.c_longlong, [c_voidp, c_int, c_int, c_int, c_int, c_int, ctypes.c_char_p,
+                                                c_size]),
     "rsgpu_update": (c_int, [c_voidp, c_voidp, c_voidp, c_size]),
     "rsgpu_split_plan": (c_int, [c_voidp, c_size, c_size, c_voidp, c_voidp]),
     "rsgpu_split": (c_int, [c_voidp, c_voidp, c_size, c_size, c_voidp, c_size, c_voidp, c_voidp]),

@@ -10,6 +10,7 @@
 #include <string>
 
 #include "rsgpu_internal.h"
+#include "xornet.h"
 #include "trace.h"
 
 namespace rsgpu {
@@ -847,11 +848,17 @@ int rsgpu_autotune_gf8(rsgpu_ctx *ctx, int n_in, int n_out, size_t nbytes, int m
     // Warm every variant first (module loading, occupancy queries), then time
     // interleaved rounds and keep each variant's fastest round, so a host or
     // device hiccup during one round cannot decide the choice.
-    for (int v = 0; v < kNumVariants; v++) RS_CUDA(launch_gf8_tile(ctx->stream, ctx->info, a, mode, v));
+    // The XOR-network variant is timed only when its kernel for this tile
+    // compiles and covers the whole size (1 KiB chunks).
+    const bool xn = nbytes >= (size_t)kXornetChunk && xornet_prepare(a, mode);
+    auto skip = [&](int v) { return v == kVariantXorNet && !xn; };
+    for (int v = 0; v < kNumVariants; v++)
+        if (!skip(v)) RS_CUDA(launch_gf8_tile(ctx->stream, ctx->info, a, mode, v));
     RS_CUDA(cudaStreamSynchronize(ctx->stream));
     std::vector<float> best_round(kNumVariants, 1e30f);
     for (int round = 0; round < 3; round++)
         for (int v = 0; v < kNumVariants; v++) {
+            if (skip(v)) continue;
             RS_CUDA(cudaEventRecord(e0, ctx->stream));
             for (int r = 0; r < reps; r++) RS_CUDA(launch_gf8_tile(ctx->stream, ctx->info, a, mode, v));
             RS_CUDA(cudaEventRecord(e1, ctx->stream));
@@ -879,6 +886,33 @@ int rsgpu_force_variant(int v) {
 }
 
 int rsgpu_num_variants(void) { return kNumVariants; }
+
+int rsgpu_record_variant(int n_in, int n_out, size_t nbytes, int mode, int variant) {
+    if (n_in <= 0 || n_in > kMaxIn || n_out <= 0 || n_out > kMaxOut || nbytes == 0 || mode < 0 ||
+        mode > kModeVerify || variant < -1 || variant >= kNumVariants)
+        return RS_ERR_INVALID_INPUT;
+    record_variant(n_in, n_out, mode, nbytes, variant);
+    return RS_OK;
+}
+
+int rsgpu_xornet_available(void) { return xornet_available() ? 1 : 0; }
+
+int rsgpu_xornet_sync(void) { return xornet_wait_idle(); }
+
+long long rsgpu_xornet_source(const uint8_t *coef, int n_in, int n_out, int mode, int group, int host,
+                              char *buf, size_t cap) {
+    if (!coef || n_in <= 0 || n_in > kMaxIn || n_out <= 0 || n_out > kXornetMaxOut || mode < 0 ||
+        mode > kModeVerify || group < 0 || group > kMaxIn)
+        return RS_ERR_INVALID_INPUT;
+    const std::string s = host ? xornet_host_source(coef, n_in, n_in, n_out, mode, group)
+                               : xornet_source(coef, n_in, n_in, n_out, mode, group);
+    if (buf && cap) {
+        const size_t n = std::min(cap - 1, s.size());
+        memcpy(buf, s.data(), n);
+        buf[n] = '\0';
+    }
+    return (long long)s.size();
+}
 
 int rsgpu_build_matrix(int kind, int k, int total, uint8_t *out) {
     if (!out) return RS_ERR_INVALID_INPUT;

@@ -43,14 +43,15 @@ enum GfVariant : int {
     kVariantFixed2 = 4, // as kVariantFixed, registers capped for 2 resident CTAs per SM
     kVariantFixed3 = 5, // as kVariantFixed, registers capped for 3 resident CTAs per SM
     kVariantFixed4 = 6, // as kVariantFixed, registers capped for 4 resident CTAs per SM
-    kNumVariants = 7,
+    kVariantXorNet = 7, // bit-sliced XOR network generated for the tile's coefficients (xornet.cpp)
+    kNumVariants = 8,
 };
 
 // Force a variant for every launch (-1 restores the tuned / default choice).
 void set_forced_variant(int v);
 int forced_variant();
 int choose_variant(int n_in, int n_out, int mode, size_t nbytes);
-void record_variant(int n_in, int n_out, int mode, size_t nbytes, int v);
+void record_variant(int n_in, int n_out, int mode, size_t nbytes, int v);  // v < 0 erases
 // Fill a parameter block for one tile (n_in <= kMaxIn, n_out <= kMaxOut).
 void fill_args(GfMatArgs &a, const uint8_t *rows, int row_stride, int n_in, int n_out,
                const uint8_t *const *in, uint8_t *const *out, size_t nbytes, int *d_flag);

@@ -28,6 +28,7 @@
 #include "gf8_device.cuh"
 #include "gf8_fixed.cuh"
 #include "kernels.h"
+#include "xornet.h"
 
 namespace rsgpu {
 namespace {
@@ -274,7 +275,9 @@ int choose_variant(int n_in, int n_out, int mode, size_t nbytes) {
 
 void record_variant(int n_in, int n_out, int mode, size_t nbytes, int v) {
     std::lock_guard<std::mutex> lk(g_mu);
-    g_tuned[std::make_tuple(n_in, (n_out + 3) / 4, mode, size_bucket(nbytes))] = v;
+    const auto key = std::make_tuple(n_in, (n_out + 3) / 4, mode, size_bucket(nbytes));
+    if (v < 0) g_tuned.erase(key);
+    else g_tuned[key] = v;
 }
 
 void fill_args(GfMatArgs &a, const uint8_t *rows, int row_stride, int ni, int no,
@@ -301,6 +304,22 @@ cudaError_t launch_gf8_tile(cudaStream_t st, const DeviceInfo &dev, const GfMatA
     for (int i = 0; i < a.n_in; i++) vec_ok &= aligned16(a.in[i]);
     for (int o = 0; o < a.n_out; o++) vec_ok &= aligned16(a.out[o]);
     long long done = 0;
+    if (variant == kVariantXorNet) {
+        // Whole 1 KiB chunks through the generated kernel (compiled on the
+        // spot when forced, else in the background); the tail, or everything
+        // while the kernel is not ready, through the default table kernel.
+        cudaError_t e = xornet_launch(st, dev, a, mode, forced_variant() == kVariantXorNet, &done);
+        if (e != cudaSuccess) return e;
+        variant = (a.n_out > 4) ? kVariantFixed2 : (mode == kModeWrite ? kVariantFixed4 : kVariantFixed3);
+        if (done == a.nbytes) return cudaGetLastError();
+        if (done > 0) {
+            GfMatArgs t = a;
+            for (int i = 0; i < a.n_in; i++) t.in[i] = a.in[i] + done;
+            for (int o = 0; o < a.n_out; o++) t.out[o] = a.out[o] + done;
+            t.nbytes = a.nbytes - done;
+            return launch_gf8_tile(st, dev, t, mode, variant);
+        }
+    }
     if (vec_ok) {
         const long long nvec = a.nbytes >> 4;
         if (nvec > 0) {

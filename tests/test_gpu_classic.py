@@ -322,14 +322,16 @@ def test_shards_past_2gib_offsets():
     torch.cuda.empty_cache()
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7])
 def test_every_kernel_variant_bit_exact(variant):
-    """Each nibble-address variant of the GF(2^8) kernel gives the oracle's bytes."""
+    """Each variant of the GF(2^8) kernel (nibble-table address forms and the
+    generated XOR network) gives the oracle's bytes."""
     lib = rs.lib()
     assert lib.rsgpu_force_variant(variant) == 0
     try:
         rng = np.random.default_rng(variant)
-        for k, p, size in [(10, 4, 4096 * 3 + 16), (17, 3, 1000), (32, 16, 2048), (5, 9, 160), (3, 1, 64)]:
+        for k, p, size in [(10, 4, 4096 * 3 + 16), (17, 3, 1000), (32, 16, 2048), (5, 9, 160), (3, 1, 64),
+                           (6, 3, 65536 + 1024 + 5), (40, 20, 3072)]:
             ref = [rng.integers(0, 256, size, dtype=np.uint8) for _ in range(k)] + \
                   [np.zeros(size, np.uint8) for _ in range(p)]
             sh = [dev(a) for a in ref]
@@ -341,6 +343,11 @@ def test_every_kernel_variant_bit_exact(variant):
             assert enc.Verify(sh)
             sh[k][size - 1] ^= 1
             assert not enc.Verify(sh)
+            sh[k][size - 1] ^= 1
+            sh[k + p - 1][0] ^= 0x80   # first chunk: inside the XOR network's range
+            assert not enc.Verify(sh)
+        if variant == 7 and lib.rsgpu_xornet_available():
+            assert lib.rsgpu_xornet_sync() >= 1
     finally:
         lib.rsgpu_force_variant(-1)
 

@@ -1,0 +1,123 @@
+"""The generated XOR-network kernel (GF(2^8) variant 7) on the device:
+bit-exact with the oracle when chosen by the tuner rather than forced, i.e.
+on first sight of a matrix (a table kernel runs while the network compiles
+in the background) and after the compile; in every mode; with a sub-chunk
+tail; for decode matrices; inside a captured batch graph."""
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+import reedsolomon_b200 as rs
+
+pytestmark = pytest.mark.gpu
+
+lib = rs.lib()
+needs_nvrtc = pytest.mark.skipif(not lib.rsgpu_xornet_available(), reason="NVRTC not loadable")
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def host(t):
+    return t.cpu().numpy()
+
+
+class tuned:
+    """Records variant 7 for the given (n_in, n_out, size, mode) geometries."""
+
+    def __init__(self, *geos):
+        self.geos = geos
+
+    def __enter__(self):
+        for ni, no, size, mode in self.geos:
+            assert lib.rsgpu_record_variant(ni, no, size, mode, 7) == 0
+
+    def __exit__(self, *exc):
+        for ni, no, size, mode in self.geos:
+            lib.rsgpu_record_variant(ni, no, size, mode, -1)
+
+
+def stripe(k, p, size, seed):
+    data = O.seeded_shards(seed, k, size)
+    want = data + [np.zeros(size, np.uint8) for _ in range(p)]
+    O.rs_encode(k, p, want)
+    return data, want
+
+
+@needs_nvrtc
+@pytest.mark.parametrize("k,p,size", [(6, 3, 65536 + 3 * 1024 + 7), (11, 5, 1 << 20), (4, 2, 1024)])
+def test_tuned_encode_first_sight_and_compiled(k, p, size):
+    data, want = stripe(k, p, size, seed=k * 100 + p)
+    enc = rs.New(k, p)
+    with tuned((k, p, size, 0), (k, p, size, 2)):
+        for rnd in range(2):   # first sight (table kernel), then the compiled network
+            sh = [dev(d) for d in data] + [torch.zeros(size, dtype=torch.uint8, device="cuda") for _ in range(p)]
+            enc.Encode(sh)
+            for i in range(k, k + p):
+                assert np.array_equal(host(sh[i]), want[i]), (rnd, i)
+            assert enc.Verify(sh)
+            sh[k + p - 1][size // 2] ^= 1
+            assert not enc.Verify(sh)
+            if rnd == 0:
+                assert lib.rsgpu_xornet_sync() >= 1
+
+
+@needs_nvrtc
+def test_tuned_reconstruct_decode_matrices():
+    k, p, size = 8, 4, 262144 + 64
+    data, want = stripe(k, p, size, seed=31)
+    enc = rs.New(k, p)
+    patterns = [(0, 9), (1, 2, 3, 11), (7,), (4, 8, 10)]
+    geos = [(k, n, size, 0) for n in (1, 2, 3, 4)]
+    with tuned(*geos):
+        for rnd in range(2):
+            for lost in patterns:
+                sh = [None if i in lost else dev(want[i]) for i in range(k + p)]
+                enc.Reconstruct(sh)
+                for i in lost:
+                    assert np.array_equal(host(sh[i]), want[i]), (rnd, lost, i)
+            lib.rsgpu_xornet_sync()
+
+
+@needs_nvrtc
+def test_xor_mode_accumulates_over_input_tiles():
+    """k > 32 splits the inputs: the first tile writes, later tiles XOR."""
+    k, p, size = 40, 3, 8192
+    data, want = stripe(k, p, size, seed=40)
+    enc = rs.New(k, p)
+    with tuned((32, p, size, 0), (8, p, size, 1)):
+        for rnd in range(2):
+            sh = [dev(d) for d in data] + [torch.full((size,), 0x5A, dtype=torch.uint8, device="cuda")
+                                           for _ in range(p)]
+            enc.Encode(sh)
+            for i in range(k, k + p):
+                assert np.array_equal(host(sh[i]), want[i]), (rnd, i)
+            lib.rsgpu_xornet_sync()
+
+
+@needs_nvrtc
+def test_batch_graph_capture_with_tuned_network():
+    """A captured batch graph runs the table kernel for a network that was
+    never loaded, and the network itself once an uncaptured launch loaded it."""
+    k, p, size, n = 5, 3, 8192, 6
+    stripes = [stripe(k, p, size, seed=500 + s) for s in range(n)]
+
+    def run(mode):
+        b = rs.Batch()
+        outs = []
+        for data, _ in stripes:
+            sh = [dev(d) for d in data] + [torch.zeros(size, dtype=torch.uint8, device="cuda") for _ in range(p)]
+            b.add_encode(k, p, sh)
+            outs.append(sh)
+        b.run(mode)
+        for (data, want), sh in zip(stripes, outs):
+            for i in range(k, k + p):
+                assert np.array_equal(host(sh[i]), want[i]), (mode, i)
+
+    with tuned((k, p, size, 0)):
+        run("graph")           # compile queued; capture used the table kernel
+        lib.rsgpu_xornet_sync()
+        run("per_stripe")      # loads the compiled network
+        run("graph")           # captured with the network

@@ -1,0 +1,123 @@
+"""The generated XOR-network schedule (variant 7 of the GF(2^8) kernel),
+checked on the CPU: librsgpu emits the same schedule the CUDA kernel runs as
+a plain C function (rs_xornet_host), one per mode; gcc compiles it and its
+outputs in the write / xor / verify modes must equal the oracle's
+codeSomeShards over random and reference encoding matrices."""
+import ctypes
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle as O
+import reedsolomon_b200 as rs
+
+pytestmark = pytest.mark.skipif(shutil.which("gcc") is None, reason="needs gcc")
+
+
+WRITE, XOR, VERIFY = 0, 1, 2
+
+
+def source(coef, mode, host, group=0):
+    lib = rs.lib()
+    coef = np.ascontiguousarray(coef, np.uint8)
+    no, ni = coef.shape
+    n = lib.rsgpu_xornet_source(coef.ctypes.data, ni, no, mode, group, host, None, 0)
+    assert n > 0
+    buf = ctypes.create_string_buffer(n + 1)
+    assert lib.rsgpu_xornet_source(coef.ctypes.data, ni, no, mode, group, host, buf, n + 1) == n
+    return buf.value.decode()
+
+
+def host_kernel(coef, mode, tmp_path, group=0):
+    c = tmp_path / ("xn%d_%d.c" % (mode, group))
+    so = tmp_path / ("xn%d_%d.so" % (mode, group))
+    c.write_text(source(coef, mode, 1, group))
+    r = subprocess.run(["gcc", "-O0", "-shared", "-fPIC", "-o", str(so), str(c)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[:2000]
+    return ctypes.CDLL(str(so))
+
+
+def run(h, ins, outs):
+    n = ins[0].size
+    assert n % 1024 == 0
+    ip = (ctypes.c_void_p * len(ins))(*[a.ctypes.data for a in ins])
+    op = (ctypes.c_void_p * len(outs))(*[a.ctypes.data for a in outs])
+    flag = ctypes.c_int(0)
+    h.rs_xornet_host(ip, op, ctypes.c_longlong(n // 1024), ctypes.byref(flag))
+    return flag.value
+
+
+def reference_parity(k, p):
+    _, m = O.build_matrix("default", k, k + p)
+    return m[k:]
+
+
+CASES = [("rs10x4", 10, 4), ("rand1x1", 1, 1), ("rand3x7", 3, 7), ("rand32x16", 32, 16),
+         ("rand17x3", 17, 3), ("rand2x16", 2, 16), ("rs6x3", 6, 3), ("rand32x8", 32, 8)]
+
+
+GROUP_CASES = [(n, i, o, 0) for n, i, o in CASES] + \
+    [("rs10x4", 10, 4, 1), ("rs10x4", 10, 4, 2), ("rand3x7", 3, 7, 1), ("rand32x8", 32, 8, 1)]
+
+
+@pytest.mark.parametrize("name,ni,no,group", GROUP_CASES)
+def test_generated_schedule_matches_oracle(name, ni, no, group, tmp_path):
+    rng = np.random.default_rng(ni * 131 + no)
+    coef = reference_parity(ni, no) if name.startswith("rs") else rng.integers(0, 256, (no, ni), dtype=np.uint8)
+    n = 3 * 1024
+    ins = [rng.integers(0, 256, n, dtype=np.uint8) for _ in range(ni)]
+    want = [np.zeros(n, np.uint8) for _ in range(no)]
+    O.code_some_shards(coef, ins, want)
+    h = host_kernel(coef, WRITE, tmp_path, group)
+    outs = [rng.integers(0, 256, n, dtype=np.uint8) for _ in range(no)]   # overwritten in write mode
+    run(h, ins, outs)
+    for j in range(no):
+        assert np.array_equal(outs[j], want[j]), (name, j)
+    h = host_kernel(coef, XOR, tmp_path, group)
+    base = [rng.integers(0, 256, n, dtype=np.uint8) for _ in range(no)]
+    acc = [b.copy() for b in base]
+    run(h, ins, acc)
+    for j in range(no):
+        assert np.array_equal(acc[j], base[j] ^ want[j]), (name, j)
+    h = host_kernel(coef, VERIFY, tmp_path, group)
+    assert run(h, ins, [w.copy() for w in want]) == 0
+    bad = [w.copy() for w in want]
+    bad[no - 1][n - 1] ^= 0x40
+    assert run(h, ins, bad) == 1
+    bad = [w.copy() for w in want]
+    bad[0][0] ^= 0x01
+    assert run(h, ins, bad) == 1
+
+
+def test_zero_and_identity_coefficients(tmp_path):
+    """Rows of zeros produce zero planes; an identity row copies its input."""
+    coef = np.zeros((3, 4), np.uint8)
+    coef[1, 2] = 1
+    coef[2, :] = [1, 1, 0, 0]
+    h = host_kernel(coef, WRITE, tmp_path)
+    rng = np.random.default_rng(9)
+    ins = [rng.integers(0, 256, 1024, dtype=np.uint8) for _ in range(4)]
+    outs = [np.full(1024, 0xFF, np.uint8) for _ in range(3)]
+    run(h, ins, outs)
+    assert not outs[0].any()
+    assert np.array_equal(outs[1], ins[2])
+    assert np.array_equal(outs[2], ins[0] ^ ins[1])
+
+
+def test_source_is_deterministic_and_bounded():
+    coef = reference_parity(10, 4)
+    a, b = source(coef, WRITE, 0), source(coef, WRITE, 0)
+    assert a == b
+    assert "rs_xornet" in a and "__launch_bounds__" in a
+    assert source(coef, VERIFY, 0) != a
+    lib = rs.lib()
+    c = np.ascontiguousarray(coef)
+    assert lib.rsgpu_xornet_source(c.ctypes.data, 33, 4, 0, 0, 0, None, 0) < 0     # more than 32 inputs
+    assert lib.rsgpu_xornet_source(c.ctypes.data, 10, 17, 0, 0, 0, None, 0) < 0    # more than 16 outputs
+    assert lib.rsgpu_xornet_source(c.ctypes.data, 10, 4, 3, 0, 0, None, 0) < 0     # no such mode
+    assert lib.rsgpu_xornet_source(c.ctypes.data, 10, 4, 0, -1, 0, None, 0) < 0    # bad group
+    small = ctypes.create_string_buffer(16)
+    n = lib.rsgpu_xornet_source(c.ctypes.data, 10, 4, 0, 0, 0, small, 16)
+    assert n == len(a) and len(small.value) == 15
