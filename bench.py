@@ -66,12 +66,16 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """DRAM bytes per launch from the committed ncu summary of this workload, if any."""
+def profile_traffic(variant):
+    """DRAM bytes per launch from the committed ncu summary of this workload
+    for the kernel that ran (the XOR network, variant 7, or a table kernel)."""
     p = os.path.join(ROOT, "profiles", "gf8_encode_rs10x4_64MiB.json")
     if os.path.exists(p):
         with open(p) as f:
-            return json.load(f).get("dram_bytes_per_launch")
+            d = json.load(f)
+        if variant != 7:
+            d = d.get("table_kernel_capture", {})
+        return d.get("dram_bytes_per_launch")
     return None
 
 
@@ -710,7 +714,9 @@ def run_ours(args):
                        "parallelism": "independent stripes per GPU"},
             "reference_convention_GBps": round(world * (k + p) * S / (ms_step / 1e3) / 1e9, 3),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": profile_traffic(),
+                         "frac": round(achieved / peak, 4),
+                         "traffic": profile_traffic(args.variant if args.variant >= 0 else best.value)
+                         if S == 64 << 20 else None,
                          "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
                          "algorithmic_bytes_per_launch": (k + p) * S},
             "e2e": None if e2e is None else {
