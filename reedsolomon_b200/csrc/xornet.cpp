@@ -311,7 +311,9 @@ struct Nvrtc {
     decltype(&nvrtcGetProgramLog) log = nullptr;
     decltype(&nvrtcDestroyProgram) destroy = nullptr;
     Nvrtc() {
+        // RSGPU_NVRTC: a path to load instead, or "off" (no XOR-network kernels).
         const char *env = getenv("RSGPU_NVRTC");
+        if (env && strcmp(env, "off") == 0) return;
         const char *names[] = {env, "libnvrtc.so.12", "libnvrtc.so"};
         void *h = nullptr;
         for (const char *n : names)

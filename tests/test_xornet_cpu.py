@@ -121,3 +121,50 @@ def test_source_is_deterministic_and_bounded():
     small = ctypes.create_string_buffer(16)
     n = lib.rsgpu_xornet_source(c.ctypes.data, 10, 4, 0, 0, 0, small, 16)
     assert n == len(a) and len(small.value) == 15
+
+
+def _nvrtc():
+    try:
+        return ctypes.CDLL("libnvrtc.so.12")
+    except OSError:
+        return None
+
+
+@pytest.mark.skipif(_nvrtc() is None, reason="libnvrtc.so.12 not loadable")
+@pytest.mark.parametrize("ni,no,mode,group", [(10, 4, WRITE, 0), (10, 4, VERIFY, 0), (10, 4, XOR, 0),
+                                              (17, 3, WRITE, 2), (32, 16, WRITE, 1), (5, 9, VERIFY, 0)])
+def test_generated_cuda_compiles_for_sm100a(ni, no, mode, group):
+    """The device form of the same schedule goes through NVRTC for sm_100a
+    (no GPU needed) and exports the kernel the library loads."""
+    nv = _nvrtc()
+    rng = np.random.default_rng(ni + 7 * no)
+    coef = reference_parity(ni, no) if (ni, no) == (10, 4) else rng.integers(0, 256, (no, ni), dtype=np.uint8)
+    src = source(coef, mode, 0, group).encode()
+    prog = ctypes.c_void_p()
+    assert nv.nvrtcCreateProgram(ctypes.byref(prog), src, b"rs_xornet.cu", 0, None, None) == 0
+    opts = [b"--gpu-architecture=sm_100a", b"--std=c++17", b"-default-device"]
+    rc = nv.nvrtcCompileProgram(prog, len(opts), (ctypes.c_char_p * len(opts))(*opts))
+    n = ctypes.c_size_t()
+    nv.nvrtcGetProgramLogSize(prog, ctypes.byref(n))
+    log = ctypes.create_string_buffer(n.value)
+    nv.nvrtcGetProgramLog(prog, log)
+    assert rc == 0, log.value.decode()[:2000]
+    size = ctypes.c_size_t()
+    assert nv.nvrtcGetCUBINSize(prog, ctypes.byref(size)) == 0 and size.value > 0
+    nv.nvrtcDestroyProgram(ctypes.byref(prog))
+
+
+def test_nvrtc_switch_off_disables_variant_7():
+    """RSGPU_NVRTC=off: no XOR-network kernels; the library still loads and
+    reports the variant unavailable (the table kernels then run)."""
+    import os
+    import sys
+    code = ("import reedsolomon_b200 as rs; l = rs.lib(); "
+            "print(l.rsgpu_xornet_available(), l.rsgpu_xornet_sync())")
+    env = dict(os.environ, RSGPU_NVRTC="off")
+    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert r.stdout.split() == ["0", "0"]
+    env["RSGPU_NVRTC"] = ""
+    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and r.stdout.split()[0] == ("1" if _nvrtc() else "0")
