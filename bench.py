@@ -49,7 +49,7 @@ def parse():
                     help="shard size; the headline workload is 64 MiB")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the secondary measurements (verify, reconstruct, batch, leopard)")
-    ap.add_argument("--extras", default="verify,reconstruct,progressive,stream,batch,leopard,serving",
+    ap.add_argument("--extras", default="c1,verify,reconstruct,progressive,stream,batch,leopard,serving",
                     help="comma list of secondary measurements to run")
     ap.add_argument("--batch-stripes", type=int, default=4096)
     ap.add_argument("--variant", type=int, default=-1,
@@ -439,6 +439,71 @@ def extra_progressive(enc, shards, S, reps=5):
             "decode_idx_data_GBps": round(k * S / (min(ms_d[1:]) / 1e3) / 1e9, 1), "decode_idx_bit_exact": ok}
 
 
+def extra_c1(dev, reps=200):
+    """RS(10,3) x 1 MiB (the reference's CPU-runnable case): per-call latency
+    of the synchronous C-ABI entry points with device shards (Encode, Verify,
+    Reconstruct of {3,7,11} checked against the original bytes), the encode
+    kernel's device time, and Encode through pinned host buffers (H2D 10 MiB +
+    D2H 3 MiB inside the call).  Launch-latency bound: ~2 us of HBM time."""
+    import ctypes
+    import time
+    import torch
+    import reedsolomon_b200 as rs
+    k, p, S = 10, 3, 1 << 20
+    lib = rs.lib()
+    enc = rs.New(k, p, rs.WithGPU(dev.index or 0))
+    g = torch.Generator(device=dev).manual_seed(1013)
+    sh = [torch.randint(0, 256, (S,), dtype=torch.uint8, device=dev, generator=g) for _ in range(k)]
+    sh += [torch.empty(S, dtype=torch.uint8, device=dev) for _ in range(p)]
+    ptrs = rs._lib.ptr_array([s.data_ptr() for s in sh])
+    ok = ctypes.c_int()
+
+    def lat(fn):
+        fn()
+        xs = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            fn()
+            xs.append((time.perf_counter() - t0) * 1e6)
+        return round(_pct(xs, 50), 1), round(_pct(xs, 99), 1)
+
+    enc_lat = lat(lambda: rs.encoder.check(lib.rsgpu_encode(enc._h, ptrs, S)))
+    ver_lat = lat(lambda: rs.encoder.check(lib.rsgpu_verify(enc._h, ptrs, S, ctypes.byref(ok))))
+    verified = bool(ok.value)
+    stream = torch.cuda.current_stream(dev)
+    enc.ctx.bind_current_stream()
+    a, b = _ev(), _ev()
+    a.record(stream)
+    for _ in range(reps):
+        lib.rsgpu_encode_async(enc._h, ptrs, S)
+    b.record(stream)
+    b.synchronize()
+    dev_us = a.elapsed_time(b) * 1e3 / reps
+    lost = (3, 7, 11)
+    keep = [sh[i].clone() for i in lost]
+    present = rs._lib.u8_array([0 if i in lost else 1 for i in range(k + p)])
+
+    def rec():
+        for i in lost:
+            sh[i].zero_()
+        rs.encoder.check(lib.rsgpu_reconstruct(enc._h, ptrs, present, S, None))
+
+    rec_lat = lat(rec)
+    rec_ok = all(torch.equal(sh[i], keep[j]) for j, i in enumerate(lost))
+    hs = [torch.empty(S, dtype=torch.uint8, pin_memory=True) for _ in range(k + p)]
+    for i in range(k):
+        hs[i].copy_(sh[i])
+    hptrs = rs._lib.ptr_array([h.data_ptr() for h in hs])
+    host_lat = lat(lambda: rs.encoder.check(lib.rsgpu_encode_host(enc._h, hptrs, S)))
+    host_ok = all(torch.equal(hs[i].to(dev), sh[i]) for i in range(k, k + p))
+    return {"geometry": "RS(10,3) x 1 MiB", "calls": reps,
+            "encode_us_p50_p99": enc_lat, "encode_kernel_us": round(dev_us, 2),
+            "encode_data_GBps_at_p50": round(k * S / (enc_lat[0] / 1e6) / 1e9, 1),
+            "verify_us_p50_p99": ver_lat, "verify_ok": verified,
+            "reconstruct_3_us_p50_p99": rec_lat, "reconstruct_bit_exact": rec_ok,
+            "host_encode_us_p50_p99": host_lat, "host_encode_bit_exact": host_ok}
+
+
 def extra_stream(shards, S, block=4 << 20):
     """StreamEncoder.Encode of the RS(10,4) stripe from in-memory readers
     (readinto into the pinned block) to in-memory writers, wall-clock timed:
@@ -700,6 +765,8 @@ def run_ours(args):
             extras["progressive"] = extra_progressive(enc, shards, S)
         if "stream" in want:
             extras["stream"] = extra_stream(shards, S)
+        if "c1" in want:
+            extras["c1"] = extra_c1(dev)
         if "serving" in want:
             extras["serving"] = extra_serving(dev)
     out = None

@@ -116,6 +116,10 @@ int rsgpu_encoder_free(rsgpu_encoder *enc);
 /* DataShards / ParityShards / TotalShards / ShardSizeMultiple (reedsolomon.go:141-165) */
 int rsgpu_encoder_info(const rsgpu_encoder *enc, int *data_shards, int *parity_shards,
                        int *shard_size_multiple, int *codec);
+/* Leopard encoders: how many erasure patterns have their error locators
+ * cached on the device (at most 256; the reference caches GF(2^8) ones,
+ * leopard8.go:465-513).  0 for classic encoders. */
+int rsgpu_leopard_errloc_cached(const rsgpu_encoder *enc);
 /* The (k+p) x k encoding matrix of a classic encoder (reedSolomon.m). */
 int rsgpu_encoder_matrix(const rsgpu_encoder *enc, uint8_t *out);
 

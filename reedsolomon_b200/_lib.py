@@ -107,6 +107,7 @@ SIGNATURES = {
     "rsgpu_autotune_gf8": (c_int, [c_voidp, c_int, c_int, c_size, c_int, c_int, c_voidp, c_intp]),
     "rsgpu_force_variant": (c_int, [c_int]),
     "rsgpu_num_variants": (c_int, []),
+    "rsgpu_leopard_errloc_cached": (c_int, [c_voidp]),
     "rsgpu_record_variant": (c_int, [c_int, c_int, c_size, c_int, c_int]),
     "rsgpu_xornet_available": (c_int, []),
     "rsgpu_xornet_sync": (c_int, []),

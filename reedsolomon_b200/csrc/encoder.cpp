@@ -403,6 +403,11 @@ int rsgpu_encoder_free(rsgpu_encoder *enc) {
     return RS_OK;
 }
 
+int rsgpu_leopard_errloc_cached(const rsgpu_encoder *enc) {
+    if (!enc || enc->codec == RS_CODEC_CLASSIC) return 0;
+    return leo_errloc_cached(enc);
+}
+
 int rsgpu_encoder_info(const rsgpu_encoder *enc, int *k, int *p, int *mult, int *codec) {
     if (!enc) return RS_ERR_INVALID_INPUT;
     if (k) *k = enc->k;

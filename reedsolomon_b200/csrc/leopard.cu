@@ -21,6 +21,9 @@
 // 128-byte line per warp.
 #include <algorithm>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <vector>
 
 #include "leo_host.h"
 #include "rsgpu_internal.h"
@@ -56,8 +59,44 @@ struct LeoState {
     }
 };
 
+// Error locators per erasure pattern (the reference caches GF(2^8) ones,
+// leopard8.go:465-513): device arrays of n entries keyed by the present-shard
+// bitmask, each with an event recorded after the kernel that filled it, so a
+// decode on any stream waits for it.  Entries are never evicted (a decode in
+// flight may read any of them); past kErrLocCacheCap patterns the locators
+// are computed per call.  Freed when the encoder is freed, after the device
+// is idle.
+struct LeoErrLocCache {
+    int device = -1;
+    std::mutex mu;
+    struct Entry {
+        uint16_t *d = nullptr;
+        cudaEvent_t ready = nullptr;
+    };
+    std::map<std::vector<uint32_t>, Entry> map;
+    ~LeoErrLocCache() {
+        if (map.empty()) return;
+        int prev = 0;
+        cudaGetDevice(&prev);
+        cudaSetDevice(device);
+        cudaDeviceSynchronize();
+        for (auto &kv : map) {
+            cudaFree(kv.second.d);
+            cudaEventDestroy(kv.second.ready);
+        }
+        cudaSetDevice(prev);
+    }
+};
+
+int leo_errloc_cached(const rsgpu_encoder *enc) {
+    if (!enc->errlocs) return 0;
+    std::lock_guard<std::mutex> lk(enc->errlocs->mu);
+    return (int)enc->errlocs->map.size();
+}
+
 namespace {
 
+constexpr size_t kErrLocCacheCap = 256;
 constexpr int kT16Stride = 256;  // u16 entries per log value (512 bytes, 4 L1 lines)
 
 struct LeoEncArgs {
@@ -1067,9 +1106,29 @@ int leo_reconstruct_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, const ui
         }
     }
     if (!st) st = enc->ctx->stream;
-    // error locators on the device: stream-ordered scratch, freed behind the decode
+    // error locators: from the per-pattern cache, else computed on the device
+    // into stream-ordered scratch (kept in the cache while it has room, else
+    // freed behind the decode)
+    if (!enc->errlocs) {
+        enc->errlocs = std::make_shared<LeoErrLocCache>();
+        enc->errlocs->device = enc->ctx->device;
+    }
+    LeoErrLocCache &cache = *enc->errlocs;
+    const std::vector<uint32_t> key(a->present, a->present + (enc->total + 31) / 32);
     uint16_t *d_el = nullptr;
-    RS_CUDA(cudaMallocFromPoolAsync((void **)&d_el, (size_t)n * sizeof(uint16_t), enc->ctx->pool, st));
+    {
+        std::lock_guard<std::mutex> lk(cache.mu);
+        auto it = cache.map.find(key);
+        if (it != cache.map.end()) {
+            d_el = it->second.d;
+            RS_CUDA(cudaStreamWaitEvent(st, it->second.ready, 0));
+        }
+    }
+    bool owned = false;  // true: scratch to free after the decode
+    if (!d_el) {
+        RS_CUDA(cudaMallocFromPoolAsync((void **)&d_el, (size_t)n * sizeof(uint16_t), enc->ctx->pool, st));
+        owned = true;
+    }
     LeoErrArgs ea;
     memset(&ea, 0, sizeof ea);
     memcpy(ea.present, a->present, sizeof ea.present);
@@ -1079,12 +1138,26 @@ int leo_reconstruct_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, const ui
     ea.n = (int)n;
     ea.out = d_el;
     ea.fold = (g16 ? enc->leo->fold16 : enc->leo->fold8) + n;
-    if (g16) leo_errloc_kernel<16><<<1, kErrLocThreads, 0, st>>>(ea);
-    else leo_errloc_kernel<8><<<1, kErrLocThreads, 0, st>>>(ea);
-    if (rc == RS_OK) rc = cuda_status(cudaGetLastError(), "leo_errloc_kernel");
-    if (rc) {
-        cudaFreeAsync(d_el, st);
-        return rc;
+    if (owned) {
+        if (g16) leo_errloc_kernel<16><<<1, kErrLocThreads, 0, st>>>(ea);
+        else leo_errloc_kernel<8><<<1, kErrLocThreads, 0, st>>>(ea);
+        rc = cuda_status(cudaGetLastError(), "leo_errloc_kernel");
+        if (rc) {
+            cudaFreeAsync(d_el, st);
+            return rc;
+        }
+        std::lock_guard<std::mutex> lk(cache.mu);
+        if (cache.map.size() < kErrLocCacheCap && !cache.map.count(key)) {
+            cudaEvent_t ev = nullptr;
+            if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess) {
+                if (cudaEventRecord(ev, st) == cudaSuccess) {
+                    cache.map[key] = LeoErrLocCache::Entry{d_el, ev};
+                    owned = false;
+                } else {
+                    cudaEventDestroy(ev);
+                }
+            }
+        }
     }
     a->errloc = d_el;
     a->k = k;
@@ -1105,7 +1178,7 @@ int leo_reconstruct_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, const ui
         else leo_decode_kernel<F8><<<grid, kLeoDecodeThreads, smem, st>>>(*a);
         rc = cuda_status(cudaGetLastError(), "leo_decode_kernel");
     }
-    cudaFreeAsync(d_el, st);
+    if (owned) cudaFreeAsync(d_el, st);
     return rc;
 }
 

@@ -23,7 +23,8 @@ int cuda_status(cudaError_t e, const char *what);
         if (_e != cudaSuccess) return cuda_status(_e, #call); \
     } while (0)
 
-struct LeoState;  // leopard.cu
+struct LeoState;        // leopard.cu
+struct LeoErrLocCache;  // leopard.cu
 
 // Grow-only device buffer owned by a context.
 struct DeviceBuffer {
@@ -60,6 +61,7 @@ struct rsgpu_encoder {
     std::vector<uint8_t> parity_rows;     // p x k
     std::unique_ptr<rsgpu::InversionTree> tree;
     std::shared_ptr<rsgpu::LeoState> leo;
+    std::shared_ptr<rsgpu::LeoErrLocCache> errlocs;  // Leopard error locators per erasure pattern
 };
 
 namespace rsgpu {
@@ -73,6 +75,7 @@ int leo_encode(rsgpu_encoder *enc, uint8_t *const *shards, size_t size);
 int leo_verify(rsgpu_encoder *enc, uint8_t *const *shards, size_t size, int *ok);
 int leo_reconstruct(rsgpu_encoder *enc, uint8_t **shards, const uint8_t *present, size_t size,
                     int recover_all, uint8_t *written);
+int leo_errloc_cached(const rsgpu_encoder *enc);  // cached erasure patterns
 // Enqueue-only variants on the context stream (no host synchronisation);
 // all shard pointers must be valid device buffers of `size` bytes.
 int leo_encode_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, size_t size, cudaStream_t st = nullptr);

@@ -189,3 +189,32 @@ def test_leopard_shards_past_2gib_offsets(gf):
         assert np.array_equal(host(cp[4][off:off + 4096]), keep[off][4])
     del sh, cp
     torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("gf", [16, 8])
+def test_errloc_cache_repeats_and_overflow(gf):
+    """Error locators are cached per erasure pattern (at most 256): repeats
+    hit the cache, patterns past the cap are computed per call, and every
+    reconstruction stays bit-exact."""
+    k, p, size = (40, 20, 128) if gf == 16 else (30, 10, 128)
+    rng = np.random.default_rng(900 + gf)
+    ref = [rng.integers(0, 256, size, dtype=np.uint8) for _ in range(k)] + \
+          [np.zeros(size, np.uint8) for _ in range(p)]
+    assert O.leo_encode(gf, k, p, ref) == 0
+    enc = new(gf, k, p)
+    lib = rs.lib()
+    assert lib.rsgpu_leopard_errloc_cached(enc._h) == 0
+    seen, pats = set(), []
+    while len(pats) < 300:
+        lost = tuple(sorted(int(x) for x in rng.choice(k + p, size=int(rng.integers(1, p + 1)), replace=False)))
+        if lost not in seen:
+            seen.add(lost)
+            pats.append(lost)
+    for rnd, batch in enumerate([pats, pats[:10], pats[-5:]]):
+        for lost in batch:
+            sh = [None if i in lost else dev(ref[i]) for i in range(k + p)]
+            enc.Reconstruct(sh)
+            for i in lost:
+                assert np.array_equal(host(sh[i]), ref[i]), (rnd, lost, i)
+        assert lib.rsgpu_leopard_errloc_cached(enc._h) == 256
+    assert lib.rsgpu_leopard_errloc_cached(rs.New(4, 2)._h) == 0
