@@ -265,10 +265,15 @@ int choose_variant(int n_in, int n_out, int mode, size_t nbytes) {
     if (g_forced >= 0) return g_forced;
     auto it = g_tuned.find(std::make_tuple(n_in, (n_out + 3) / 4, mode, size_bucket(nbytes)));
     if (it != g_tuned.end()) return it->second;
-    // Untuned default: the unrolled kernel with the most resident warps that
+    // Untuned default: the generated XOR network from 256 KiB per shard when
+    // NVRTC is present (faster than every table kernel at 16 MiB and above in
+    // all measured geometries, and at 1 MiB with enough SMs covered; the
+    // first launches of a new matrix run a table kernel while it compiles).
+    // Otherwise the unrolled table kernel with the most resident warps that
     // does not spill (up to 4 outputs: 4 CTAs per SM when writing, 3 when the
     // outputs are also read, which holds them in registers; 2 for 5-8
     // outputs); input counts without a specialisation fall back to kVariantPrmt.
+    if (nbytes >= kXornetDefaultMin && xornet_available()) return kVariantXorNet;
     if (n_out > 4) return kVariantFixed2;
     return mode == kModeWrite ? kVariantFixed4 : kVariantFixed3;
 }

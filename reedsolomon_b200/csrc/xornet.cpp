@@ -384,11 +384,14 @@ struct Key {
 };
 
 struct Entry {
-    enum State { kQueued, kCompiled, kFailed } state = kQueued;
+    // kQueued: waiting in the queue; kCompiling: a worker or a synchronous
+    // caller is compiling it; kCompiled / kFailed: final.
+    enum State { kQueued, kCompiling, kCompiled, kFailed } state = kQueued;
+    bool final_state() const { return state == kCompiled || state == kFailed; }
     std::vector<char> cubin;
     cudaLibrary_t lib = nullptr;
     cudaKernel_t kern = nullptr;
-    int blocks_per_sm[64] = {};  // per device ordinal, 0 = not queried
+    int blocks_per_sm[64][5] = {};  // [device ordinal][log2 warps per CTA], 0 = not queried
 };
 
 struct Cache {
@@ -436,6 +439,7 @@ void worker_loop() {
             c.cv.wait(lk, [&] { return !c.queue.empty(); });
             job = std::move(c.queue.front());
             c.queue.pop_front();
+            job.second->state = Entry::kCompiling;
             c.busy++;
         }
         std::vector<char> bin = build_kernel(job.first);
@@ -481,12 +485,23 @@ std::shared_ptr<Entry> lookup(const GfMatArgs &a, int mode, bool sync) {
     Key key = make_key(a, mode);
     std::shared_ptr<Entry> e;
     {
-        std::lock_guard<std::mutex> lk(c.mu);
+        std::unique_lock<std::mutex> lk(c.mu);
         auto it = c.map.find(key);
         if (it != c.map.end()) {
             e = it->second;
             if (e->state == Entry::kCompiled) return e;
-            if (e->state == Entry::kFailed) return nullptr;
+            if (e->state == Entry::kFailed || !sync) return nullptr;
+            if (e->state == Entry::kCompiling) {
+                // someone else is compiling this entry: wait for them
+                c.idle.wait(lk, [&] { return e->final_state(); });
+                return e->state == Entry::kCompiled ? e : nullptr;
+            }
+            // still queued: take it out of the queue and compile it here
+            for (auto q = c.queue.begin(); q != c.queue.end(); ++q)
+                if (q->second == e) {
+                    c.queue.erase(q);
+                    break;
+                }
         } else if (c.map.size() >= (size_t)kXornetCacheCap) {
             return nullptr;
         } else {
@@ -505,24 +520,15 @@ std::shared_ptr<Entry> lookup(const GfMatArgs &a, int mode, bool sync) {
                 return nullptr;
             }
         }
-    }
-    if (!sync) return nullptr;
-    {
-        // Queued for the worker already: wait for it.
-        std::unique_lock<std::mutex> lk(c.mu);
-        const bool queued = std::any_of(c.queue.begin(), c.queue.end(),
-                                        [&](const std::pair<Key, std::shared_ptr<Entry>> &q) { return q.second == e; });
-        if (queued || c.busy) {
-            c.idle.wait(lk, [&] { return e->state != Entry::kQueued; });
-            return e->state == Entry::kCompiled ? e : nullptr;
-        }
+        e->state = Entry::kCompiling;
     }
     std::vector<char> bin = build_kernel(key);
-    std::lock_guard<std::mutex> lk(c.mu);
-    if (e->state == Entry::kQueued) {
+    {
+        std::lock_guard<std::mutex> lk(c.mu);
         e->cubin = std::move(bin);
         e->state = e->cubin.empty() ? Entry::kFailed : Entry::kCompiled;
     }
+    c.idle.notify_all();
     return e->state == Entry::kCompiled ? e : nullptr;
 }
 
@@ -562,7 +568,13 @@ cudaError_t xornet_launch(cudaStream_t st, const DeviceInfo &dev, const GfMatArg
         if (reinterpret_cast<uintptr_t>(a.out[o]) & 15u) return cudaSuccess;
     std::shared_ptr<Entry> e = lookup(a, mode, sync);
     if (!e) return cudaSuccess;
-    const int threads = xornet_threads(a.n_out);
+    // Warps per CTA: the compiled maximum, halved while that would leave SMs
+    // without work (1 MiB shards are 1024 warp steps: 4-warp CTAs spread
+    // them over every SM where 16-warp CTAs would fill 64).
+    int lw = 0;
+    while ((32 << (lw + 1)) <= xornet_threads(a.n_out)) lw++;
+    while (lw > 0 && nchunk < (long long)dev.sm_count << lw) lw--;
+    const int threads = 32 << lw;
     cudaKernel_t kern;
     int nb;
     {
@@ -579,7 +591,7 @@ cudaError_t xornet_launch(cudaStream_t st, const DeviceInfo &dev, const GfMatArg
             if (rc != cudaSuccess) return rc;
         }
         kern = e->kern;
-        int &slot = e->blocks_per_sm[dev.device & 63];
+        int &slot = e->blocks_per_sm[dev.device & 63][lw];
         if (slot == 0) {
             int q = 0;
             if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&q, (const void *)kern, threads, 0) !=

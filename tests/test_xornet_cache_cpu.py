@@ -1,0 +1,41 @@
+"""Concurrency of the XOR-network compile cache, on the CPU: background
+compiles queued through the launch path (which returns before any CUDA call
+while a matrix is not compiled) race synchronous compiles of the same and of
+new matrices.  The harness (tests/xornet_cache_stress.cpp) links the
+library's internal C++ entry points and must finish without deadlock, with
+every synchronous compile succeeding."""
+import ctypes
+import os
+import shutil
+import subprocess
+
+import pytest
+
+import reedsolomon_b200 as rs
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+PKG = os.path.join(ROOT, "reedsolomon_b200")
+CUDA_INC = "/usr/local/cuda/include"
+
+
+def _nvrtc():
+    try:
+        ctypes.CDLL("libnvrtc.so.12")
+        return True
+    except OSError:
+        return False
+
+
+@pytest.mark.skipif(shutil.which("g++") is None or not os.path.isdir(CUDA_INC) or not _nvrtc(),
+                    reason="needs g++, CUDA headers and libnvrtc")
+def test_sync_and_background_compiles_do_not_deadlock(tmp_path):
+    rs.lib()  # built
+    exe = tmp_path / "stress"
+    r = subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(PKG, "csrc"), "-I", os.path.join(ROOT, "include"),
+                        "-I", CUDA_INC, os.path.join(HERE, "xornet_cache_stress.cpp"), "-o", str(exe),
+                        "-L", PKG, "-lrsgpu", "-Wl,-rpath," + PKG, "-lpthread"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "bad=0" in r.stdout
