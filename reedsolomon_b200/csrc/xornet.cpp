@@ -23,11 +23,12 @@
 //   * transposes the accumulators back and stores them (or XORs into the
 //     outputs, or compares with them for verification).
 //
-// Per input byte of RS(10,4) this costs about 3.4 integer instructions and
-// no shared-memory lookups, against 3.9 ALU instructions and two lookups for
-// the nibble-table kernel, whose shared-memory pipe saturates first.  Kernels are cached per (n_in, n_out, coefficients); a
-// matrix that is not compiled yet is queued for a background compile and the
-// caller runs a table kernel meanwhile.
+// Per input byte of RS(10,4) this runs about 4.9 integer instructions (all
+// on the ALU and FMA pipes) and no shared-memory lookups; the nibble-table
+// kernel needs two lookups per byte and saturates the shared-memory pipe
+// first.  Kernels are cached per (mode, n_in, n_out, coefficients); a matrix
+// that is not compiled yet is queued for a background compile and the caller
+// runs a table kernel meanwhile.
 #include <cuda_runtime.h>
 #include <dlfcn.h>
 #include <nvrtc.h>
@@ -109,7 +110,6 @@ struct XnArgs {
     long long nchunk;
     int *flag;
 };
-// Exchanges bits (mh) of x with bits (m) of y, mh = m << s; r = 2^(32-s), l = 2^s.
 // Exchanges bits mh = m << s of x with bits m of y (one delta swap).
 #define XN_SWAP(x, y, m, mh, s) { const u32 xs_ = (x) >> (s), ys_ = (y) << (s); \
     x = ((x) & ~(mh)) | (ys_ & (mh)); y = ((y) & ~(m)) | (xs_ & (m)); }
