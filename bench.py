@@ -795,6 +795,8 @@ def run_ours(args):
             "clocks": clk.summary(),
         }
         if not args.no_cpu_baseline and world == 1:  # rank 0 at N=1 only
+            # no background kernel compiles may share the host cores with the baseline
+            lib.rsgpu_xornet_sync()
             threads = os.cpu_count() or 1
             gbs, n, el, isa = cpu_reference(args.cpu_seconds, threads, shard=16 << 20)
             out["cpu_baseline"] = {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": "port",
