@@ -121,3 +121,50 @@ def test_batch_graph_capture_with_tuned_network():
         lib.rsgpu_xornet_sync()
         run("per_stripe")      # loads the compiled network
         run("graph")           # captured with the network
+
+
+@needs_nvrtc
+@pytest.mark.parametrize("skew", [1, 8, 16])
+def test_forced_network_with_unaligned_shards(skew):
+    """Shards off the 16-byte grid (skew 1, 8) cannot use the vector network:
+    the table kernels take over.  On the grid (skew 16) the network covers
+    the whole 1 KiB chunks and a table kernel the 5-byte tail.  Bytes around
+    every shard stay untouched."""
+    k, p, size = 6, 3, (256 << 10) + 5
+    data, want = stripe(k, p, size, seed=600 + skew)
+    pitch = (size + 64 + 15) // 16 * 16
+    buf = torch.full(((k + p) * pitch,), 0xA5, dtype=torch.uint8, device="cuda")
+    sh = [buf[i * pitch + skew: i * pitch + skew + size] for i in range(k + p)]
+    for i in range(k):
+        sh[i].copy_(dev(data[i]))
+    assert lib.rsgpu_force_variant(7) == 0
+    try:
+        enc = rs.New(k, p)
+        enc.Encode(sh)
+        for i in range(k, k + p):
+            assert np.array_equal(host(sh[i]), want[i]), i
+        assert enc.Verify(sh)
+    finally:
+        lib.rsgpu_force_variant(-1)
+    h = host(buf).reshape(k + p, pitch)
+    assert (h[:, :skew] == 0xA5).all() and (h[:, skew + size:] == 0xA5).all()
+
+
+@needs_nvrtc
+def test_forced_network_wide_tile_1mib():
+    """32 x 16 tile (256-thread kernel, smaller factoring groups) at 1 MiB,
+    where launches use fewer warps per CTA to cover every SM."""
+    k, p, size = 32, 16, 1 << 20
+    data, want = stripe(k, p, size, seed=3216)
+    assert lib.rsgpu_force_variant(7) == 0
+    try:
+        enc = rs.New(k, p)
+        sh = [dev(d) for d in data] + [torch.zeros(size, dtype=torch.uint8, device="cuda") for _ in range(p)]
+        enc.Encode(sh)
+        for i in range(k, k + p):
+            assert np.array_equal(host(sh[i]), want[i]), i
+        assert enc.Verify(sh)
+        sh[k + 7][size - 1] ^= 2
+        assert not enc.Verify(sh)
+    finally:
+        lib.rsgpu_force_variant(-1)
