@@ -204,10 +204,12 @@ int rsgpu_check_some_shards(rsgpu_ctx *ctx, const uint8_t *rows, int n_in, int n
  * context, no allocation.  Its scratch is one 8 MiB array per device, static in
  * the library and held until exit; more than 32 inputs need
  * n_out * round_up(nbytes, 256) <= 8 MiB - 256, larger calls return
- * RS_ERR_INVALID_INPUT.  Runs on `cuda_stream` on the current device and
- * waits for it.  The first call on a device looks up the array's device
- * address; make it before any stream capture.  Calls that overlap on the GPU
- * share the array and race: serialise them. */
+ * RS_ERR_INVALID_INPUT.  Only the table kernels run (the run-time compiled
+ * XOR-network kernels load a module, which allocates device memory).  Runs
+ * on `cuda_stream` on the current device and waits for it.  The first call
+ * on a device looks up the array's device address; make it before any
+ * stream capture.  Calls that overlap on the GPU share the array and race:
+ * serialise them. */
 int rsgpu_check_some_shards_noalloc(const uint8_t *rows, int n_in, int n_out,
                                     const uint8_t *const *in, const uint8_t *const *to_check,
                                     size_t nbytes, void *cuda_stream, int *ok);

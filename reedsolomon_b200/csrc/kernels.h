@@ -63,9 +63,11 @@ cudaError_t launch_gf8_tile(cudaStream_t st, const DeviceInfo &dev, const GfMatA
 // and n_out > kMaxOut.  rows is n_out x n_in row-major on the host.  For
 // kModeVerify the sum is compared with out[] and *d_flag is set on mismatch
 // (requires n_in <= kMaxIn; larger verifies are composed by the caller).
+// allow_generated = false keeps every tile on the table kernels: no run-time
+// compiled XOR-network module is loaded (a device allocation) or queued.
 cudaError_t launch_gf8_matmul(cudaStream_t st, const DeviceInfo &dev, const uint8_t *rows, int n_in,
                               int n_out, const uint8_t *const *in, uint8_t *const *out,
-                              size_t nbytes, int mode, int *d_flag);
+                              size_t nbytes, int mode, int *d_flag, bool allow_generated = true);
 
 // Fill an 8-byte aligned buffer with uniform pseudo-random bytes (tuning inputs).
 cudaError_t launch_fill_random(cudaStream_t st, const DeviceInfo &dev, uint8_t *p, size_t nbytes,

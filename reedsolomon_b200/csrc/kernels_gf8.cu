@@ -260,6 +260,14 @@ int forced_variant() {
     return g_forced;
 }
 
+namespace {
+// The untuned table-kernel choice (see choose_variant).
+int table_variant(int n_out, int mode) {
+    if (n_out > 4) return kVariantFixed2;
+    return mode == kModeWrite ? kVariantFixed4 : kVariantFixed3;
+}
+}  // namespace
+
 int choose_variant(int n_in, int n_out, int mode, size_t nbytes) {
     std::lock_guard<std::mutex> lk(g_mu);
     if (g_forced >= 0) return g_forced;
@@ -274,8 +282,7 @@ int choose_variant(int n_in, int n_out, int mode, size_t nbytes) {
     // outputs are also read, which holds them in registers; 2 for 5-8
     // outputs); input counts without a specialisation fall back to kVariantPrmt.
     if (nbytes >= kXornetDefaultMin && xornet_available()) return kVariantXorNet;
-    if (n_out > 4) return kVariantFixed2;
-    return mode == kModeWrite ? kVariantFixed4 : kVariantFixed3;
+    return table_variant(n_out, mode);
 }
 
 void record_variant(int n_in, int n_out, int mode, size_t nbytes, int v) {
@@ -350,7 +357,7 @@ cudaError_t launch_gf8_tile(cudaStream_t st, const DeviceInfo &dev, const GfMatA
 
 cudaError_t launch_gf8_matmul(cudaStream_t st, const DeviceInfo &dev, const uint8_t *rows, int n_in,
                               int n_out, const uint8_t *const *in, uint8_t *const *out,
-                              size_t nbytes, int mode, int *d_flag) {
+                              size_t nbytes, int mode, int *d_flag, bool allow_generated) {
     if (n_in <= 0 || n_out <= 0 || nbytes == 0) return cudaSuccess;
     for (int o0 = 0; o0 < n_out; o0 += kMaxOut) {
         const int no = std::min(kMaxOut, n_out - o0);
@@ -360,7 +367,9 @@ cudaError_t launch_gf8_matmul(cudaStream_t st, const DeviceInfo &dev, const uint
             fill_args(a, rows + (size_t)o0 * n_in + i0, n_in, ni, no, in + i0, out + o0, nbytes, d_flag);
             // Only the first input tile may overwrite; later tiles accumulate.
             const int m = (mode == kModeWrite && i0 > 0) ? kModeXor : mode;
-            cudaError_t e = launch_gf8_tile(st, dev, a, m, choose_variant(ni, no, m, nbytes));
+            int v = choose_variant(ni, no, m, nbytes);
+            if (!allow_generated && v == kVariantXorNet) v = table_variant(no, m);
+            cudaError_t e = launch_gf8_tile(st, dev, a, m, v);
             if (e != cudaSuccess) return e;
         }
     }

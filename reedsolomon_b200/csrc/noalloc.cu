@@ -24,6 +24,9 @@ namespace {
 constexpr size_t kNoAllocScratchBytes = 8u << 20;  // per device
 constexpr size_t kFlagBytes = 256;                 // mismatch flag, padded to keep rows aligned
 constexpr int kMaxDevices = 64;
+// Only the table kernels: the run-time compiled XOR-network kernels load a
+// module on first use, which allocates device memory.
+constexpr bool kTableKernelsOnly = false;
 
 __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocScratchBytes];
 
@@ -86,7 +89,7 @@ extern "C" int rsgpu_check_some_shards_noalloc(const uint8_t *rows, int n_in, in
     RS_CUDA(cudaMemsetAsync(d_flag, 0, sizeof(int), st));
     if (n_in <= kMaxIn) {
         RS_CUDA(launch_gf8_matmul(st, info, rows, n_in, n_out, in, const_cast<uint8_t *const *>(to_check),
-                                  nbytes, kModeVerify, d_flag));
+                                  nbytes, kModeVerify, d_flag, kTableKernelsOnly));
     } else {
         uint8_t *tmp[kMaxOut];
         for (int o0 = 0; o0 < n_out; o0 += kMaxOut) {
@@ -95,12 +98,13 @@ extern "C" int rsgpu_check_some_shards_noalloc(const uint8_t *rows, int n_in, in
             const int no = n_out - o0 < kMaxOut ? n_out - o0 : kMaxOut;
             for (int o = 0; o < no; o++) tmp[o] = scratch + kFlagBytes + pitch * (size_t)(o0 + o);
             RS_CUDA(launch_gf8_matmul(st, info, rows + (size_t)o0 * n_in, n_in, no, in, tmp, nbytes,
-                                      kModeWrite, d_flag));
+                                      kModeWrite, d_flag, kTableKernelsOnly));
             const uint8_t one = 1;
             for (int o = 0; o < no; o++) {
                 const uint8_t *src = tmp[o];
                 uint8_t *chk = const_cast<uint8_t *>(to_check[o0 + o]);
-                RS_CUDA(launch_gf8_matmul(st, info, &one, 1, 1, &src, &chk, nbytes, kModeVerify, d_flag));
+                RS_CUDA(launch_gf8_matmul(st, info, &one, 1, 1, &src, &chk, nbytes, kModeVerify, d_flag,
+                                          kTableKernelsOnly));
             }
         }
     }

@@ -72,3 +72,33 @@ def test_noalloc_rejects_scratch_overflow():
                                              ctypes.byref(ok))
     assert rc == -8
     assert b"8 MiB" in lib.rsgpu_last_error()
+
+
+def test_noalloc_runs_table_kernels_only():
+    """Large shards default to kernels compiled at run time, whose first
+    launch loads a module (a device allocation): the no-alloc entry point
+    must never queue or load one, even with that variant forced."""
+    lib = L.lib()
+    rng = np.random.default_rng(77)
+    k, p, size = 6, 3, 512 << 10
+    rows = rng.integers(1, 256, (p, k), dtype=np.uint8)   # a matrix no other test uses
+    data = [rng.integers(0, 256, size, dtype=np.uint8) for _ in range(k)]
+    par = [np.zeros(size, np.uint8) for _ in range(p)]
+    O.code_some_shards(rows, data, par)
+    ins = [torch.from_numpy(d).cuda() for d in data]
+    chk = [torch.from_numpy(x).cuda() for x in par]
+    pi = L.ptr_array([t.data_ptr() for t in ins])
+    pc = L.ptr_array([t.data_ptr() for t in chk])
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    before = lib.rsgpu_xornet_sync()
+    for forced in (-1, 7):
+        assert lib.rsgpu_force_variant(forced) == 0
+        try:
+            for _ in range(2):
+                ok = ctypes.c_int(-1)
+                assert lib.rsgpu_check_some_shards_noalloc(rows.ctypes.data, k, p, pi, pc, size, stream,
+                                                           ctypes.byref(ok)) == 0
+                assert ok.value == 1
+        finally:
+            lib.rsgpu_force_variant(-1)
+    assert lib.rsgpu_xornet_sync() == before
