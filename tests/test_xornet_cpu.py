@@ -168,3 +168,18 @@ def test_nvrtc_switch_off_disables_variant_7():
     env["RSGPU_NVRTC"] = ""
     r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=120)
     assert r.returncode == 0 and r.stdout.split()[0] == ("1" if _nvrtc() else "0")
+
+
+def test_record_and_force_variant_arguments():
+    """The tuning records need no device: bad geometries, modes and variants
+    are refused; a recorded choice can be removed again."""
+    lib = rs.lib()
+    n = lib.rsgpu_num_variants()
+    assert n == 8
+    assert lib.rsgpu_record_variant(10, 4, 1 << 20, 0, 7) == 0
+    assert lib.rsgpu_record_variant(10, 4, 1 << 20, 0, -1) == 0
+    for args in [(0, 4, 1 << 20, 0, 7), (33, 4, 1 << 20, 0, 7), (10, 17, 1 << 20, 0, 7), (10, 4, 0, 0, 7),
+                 (10, 4, 1 << 20, 3, 7), (10, 4, 1 << 20, 0, n), (10, 4, 1 << 20, 0, -2)]:
+        assert lib.rsgpu_record_variant(*args) < 0, args
+    assert lib.rsgpu_force_variant(n) < 0
+    assert lib.rsgpu_force_variant(-1) == 0
