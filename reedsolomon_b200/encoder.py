@@ -747,6 +747,45 @@ def invert_matrix(m):
     return out
 
 
+# ---- GF(2^8) kernel variants and tuning ---------------------------------------
+MODES = {"write": 0, "xor": 1, "verify": 2}
+VARIANT_XORNET = 7  # the bit-sliced XOR network generated per coefficient matrix
+
+
+def autotune(n_in, n_out, shard_bytes, mode="write", reps=3, device=0):
+    """Times every GF(2^8) kernel variant for this geometry on scratch data
+    and keeps the fastest for its input count, output group, mode and size
+    bucket.  Returns (best variant, {variant: ms}); variants that cannot run
+    here (no NVRTC for the XOR network) are absent from the dict."""
+    lib = L.lib()
+    ms = (ctypes.c_float * lib.rsgpu_num_variants())()
+    best = ctypes.c_int(-1)
+    check(lib.rsgpu_autotune_gf8(Context.get(device).handle, n_in, n_out, shard_bytes, MODES[mode], reps, ms,
+                                 ctypes.byref(best)))
+    return best.value, {v: x for v, x in enumerate(ms) if x < 1e29}
+
+
+def record_variant(n_in, n_out, shard_bytes, variant, mode="write"):
+    """Installs a saved tuning choice without timing (None removes it)."""
+    check(L.lib().rsgpu_record_variant(n_in, n_out, shard_bytes, MODES[mode], -1 if variant is None else variant))
+
+
+def force_variant(variant):
+    """Uses one variant for every launch (None: back to the tuned choice)."""
+    check(L.lib().rsgpu_force_variant(-1 if variant is None else variant))
+
+
+def generated_kernels_available():
+    """True when the per-matrix XOR-network kernels can be compiled (NVRTC)."""
+    return bool(L.lib().rsgpu_xornet_available())
+
+
+def wait_generated_kernels():
+    """Waits for queued background compiles; returns how many generated
+    kernels this process holds."""
+    return L.lib().rsgpu_xornet_sync()
+
+
 # ---- batched mixed-geometry execution ---------------------------------------
 RS_JOB_ENCODE, RS_JOB_RECONSTRUCT, RS_JOB_RECONSTRUCT_DATA, RS_JOB_VERIFY = 0, 1, 2, 3
 BATCH_MODES = {"persistent": 0, "per_stripe": 1, "graph": 2}

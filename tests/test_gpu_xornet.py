@@ -168,3 +168,15 @@ def test_forced_network_wide_tile_1mib():
         assert not enc.Verify(sh)
     finally:
         lib.rsgpu_force_variant(-1)
+
+
+def test_python_autotune_helper():
+    """rs.autotune times every variant (the XOR network included when NVRTC
+    is present) and records the fastest; record_variant(None) removes it."""
+    best, ms = rs.autotune(10, 4, 1 << 20)
+    assert best in ms and all(v > 0 for v in ms.values())
+    assert (rs.VARIANT_XORNET in ms) == bool(lib.rsgpu_xornet_available())
+    best_v, ms_v = rs.autotune(10, 4, 1 << 20, mode="verify", reps=2)
+    assert best_v in ms_v
+    rs.record_variant(10, 4, 1 << 20, None)
+    rs.record_variant(10, 4, 1 << 20, None, mode="verify")

@@ -183,3 +183,16 @@ def test_record_and_force_variant_arguments():
         assert lib.rsgpu_record_variant(*args) < 0, args
     assert lib.rsgpu_force_variant(n) < 0
     assert lib.rsgpu_force_variant(-1) == 0
+
+
+def test_python_tuning_helpers_without_device():
+    assert rs.generated_kernels_available() == bool(_nvrtc())
+    rs.record_variant(10, 4, 1 << 20, rs.VARIANT_XORNET)
+    rs.record_variant(10, 4, 1 << 20, None)
+    rs.record_variant(10, 4, 1 << 20, 3, mode="verify")
+    rs.record_variant(10, 4, 1 << 20, None, mode="verify")
+    rs.force_variant(6)
+    rs.force_variant(None)
+    with pytest.raises(rs.RSError):
+        rs.force_variant(99)
+    assert rs.wait_generated_kernels() >= 0
