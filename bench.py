@@ -790,7 +790,9 @@ def run_ours(args):
                          "frac": round(achieved / peak, 4),
                          "traffic": profile_traffic(args.variant if args.variant >= 0 else best.value)
                          if S == 64 << 20 else None,
-                         "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
+                         "peak_kind": "measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                         else "fallback (6650 GB/s, an earlier copy measurement on these GPUs; "
+                              "MEASURED_PEAKS.json absent)",
                          "algorithmic_bytes_per_launch": (k + p) * S},
             "e2e": None if e2e is None else {
                 "value": round(e2e, 3), "unit": "GB/s", "h2d_bytes_per_step": k * S,
