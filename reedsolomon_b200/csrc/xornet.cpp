@@ -33,7 +33,11 @@
 #include <dlfcn.h>
 #include <nvrtc.h>
 
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cctype>
@@ -310,6 +314,7 @@ struct Nvrtc {
     decltype(&nvrtcGetProgramLogSize) log_size = nullptr;
     decltype(&nvrtcGetProgramLog) log = nullptr;
     decltype(&nvrtcDestroyProgram) destroy = nullptr;
+    int major = 0, minor = 0;  // nvrtcVersion, part of the on-disk cache key
     Nvrtc() {
         // RSGPU_NVRTC: a path to load instead, or "off" (no XOR-network kernels).
         const char *env = getenv("RSGPU_NVRTC");
@@ -327,6 +332,8 @@ struct Nvrtc {
         log = (decltype(log))dlsym(h, "nvrtcGetProgramLog");
         destroy = (decltype(destroy))dlsym(h, "nvrtcDestroyProgram");
         ok = create && compile && cubin_size && cubin && log_size && log && destroy;
+        auto version = (decltype(&nvrtcVersion))dlsym(h, "nvrtcVersion");
+        if (version) version(&major, &minor);
     }
 };
 
@@ -338,11 +345,14 @@ const Nvrtc &nvrtc() {
 // Compiles one generated kernel to an sm_100a cubin; empty on failure.
 // *spill receives the spill-store bytes ptxas reports (-1 if unknown).  The
 // log goes to stderr on failure when RSGPU_XORNET_LOG is set.
+std::atomic<int> g_compiles{0};  // NVRTC compilations in this process
+
 std::vector<char> compile_cubin(const std::string &src, int *spill) {
     const Nvrtc &nv = nvrtc();
     std::vector<char> out;
     *spill = -1;
     if (!nv.ok) return out;
+    g_compiles++;
     nvrtcProgram prog;
     if (nv.create(&prog, src.c_str(), "rs_xornet.cu", 0, nullptr, nullptr) != NVRTC_SUCCESS) return out;
     const char *opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "-default-device", "--ptxas-options=-v"};
@@ -413,7 +423,74 @@ Cache &cache() {
 // kernel that spills at most kSpillOk bytes (else the one that spills least).
 constexpr int kSpillOk = 128;
 
+// ---- optional on-disk cache --------------------------------------------------
+// RSGPU_KERNEL_CACHE=<directory> keeps every final cubin in a file named by a
+// 64-bit FNV-1a hash of the kernel's generated source (preferred group), the
+// NVRTC version and the target, so a new process loads it instead of
+// compiling.  A file is used only when its header (magic, hash, size)
+// matches; files are written to a temporary name and renamed into place.
+struct DiskHeader {
+    char magic[8];
+    uint64_t hash;
+    uint64_t size;
+};
+constexpr char kDiskMagic[8] = {'R', 'S', 'X', 'N', 'C', '0', '1', '\0'};
+constexpr uint64_t kDiskMaxBytes = 64ull << 20;
+
+uint64_t fnv1a(const std::string &s) {
+    uint64_t h = 0xcbf29ce484222325ull;
+    for (unsigned char c : s) {
+        h ^= c;
+        h *= 0x100000001b3ull;
+    }
+    return h;
+}
+
+bool disk_read(const std::string &path, uint64_t hash, std::vector<char> &out) {
+    FILE *f = fopen(path.c_str(), "rb");
+    if (!f) return false;
+    DiskHeader h;
+    bool ok = fread(&h, sizeof h, 1, f) == 1 && memcmp(h.magic, kDiskMagic, sizeof kDiskMagic) == 0 &&
+              h.hash == hash && h.size > 0 && h.size <= kDiskMaxBytes;
+    if (ok) {
+        out.resize(h.size);
+        ok = fread(out.data(), 1, h.size, f) == h.size && fgetc(f) == EOF;
+    }
+    fclose(f);
+    if (!ok) out.clear();
+    return ok;
+}
+
+void disk_write(const std::string &dir, const std::string &path, uint64_t hash, const std::vector<char> &bin) {
+    static std::atomic<unsigned> seq{0};
+    mkdir(dir.c_str(), 0755);  // one level; an existing directory is fine
+    const std::string tmp = path + ".tmp." + std::to_string((long)getpid()) + "." + std::to_string(seq++);
+    FILE *f = fopen(tmp.c_str(), "wb");
+    if (!f) return;
+    DiskHeader h;
+    memcpy(h.magic, kDiskMagic, sizeof kDiskMagic);
+    h.hash = hash;
+    h.size = bin.size();
+    const bool ok = fwrite(&h, sizeof h, 1, f) == 1 && fwrite(bin.data(), 1, bin.size(), f) == bin.size();
+    if (fclose(f) == 0 && ok) rename(tmp.c_str(), path.c_str());
+    else remove(tmp.c_str());
+}
+
 std::vector<char> build_kernel(const Key &k) {
+    const char *dir_env = getenv("RSGPU_KERNEL_CACHE");
+    const std::string dir = dir_env ? dir_env : "";
+    std::string path;
+    uint64_t hash = 0;
+    if (!dir.empty()) {
+        const Nvrtc &nv = nvrtc();
+        hash = fnv1a(xornet_source(k.coef.data(), k.n_in, k.n_in, k.n_out, k.mode, xornet_group(k.n_out)) +
+                     "|nvrtc " + std::to_string(nv.major) + "." + std::to_string(nv.minor) + "|sm_100a");
+        char name[48];
+        snprintf(name, sizeof name, "/rs_xornet_%016llx.cubin", (unsigned long long)hash);
+        path = dir + name;
+        std::vector<char> cached;
+        if (disk_read(path, hash, cached)) return cached;
+    }
     std::vector<char> best;
     int best_spill = 1 << 30;
     for (int g = xornet_group(k.n_out); g >= 1; g--) {
@@ -427,6 +504,7 @@ std::vector<char> build_kernel(const Key &k) {
         }
         if (best_spill <= kSpillOk) break;
     }
+    if (!path.empty() && !best.empty()) disk_write(dir, path, hash, best);
     return best;
 }
 
@@ -543,6 +621,8 @@ struct XnArgs {
 }  // namespace
 
 bool xornet_available() { return nvrtc().ok; }
+
+int xornet_compile_count() { return g_compiles.load(); }
 
 bool xornet_prepare(const GfMatArgs &a, int mode) {
     return a.n_in <= 32 && a.n_out <= kXornetMaxOut && lookup(a, mode, true) != nullptr;

@@ -25,6 +25,9 @@ int xornet_group(int n_out);
 bool xornet_available();
 // Compiles (now) the kernel for a's coefficients; false when it cannot exist.
 bool xornet_prepare(const GfMatArgs &a, int mode);
+// NVRTC compilations run by this process (kernels read from the on-disk
+// cache, RSGPU_KERNEL_CACHE, do not count).
+int xornet_compile_count();
 // Waits for queued background compiles; returns the number of compiled kernels.
 int xornet_wait_idle();
 // Runs the XOR-network kernel over the whole 1 KiB chunks of a (16-byte

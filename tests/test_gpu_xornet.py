@@ -180,3 +180,35 @@ def test_python_autotune_helper():
     assert best_v in ms_v
     rs.record_variant(10, 4, 1 << 20, None)
     rs.record_variant(10, 4, 1 << 20, None, mode="verify")
+
+
+@needs_nvrtc
+def test_disk_cached_kernels_load_and_match(tmp_path):
+    """With RSGPU_KERNEL_CACHE set, one process compiles and stores the
+    kernel, a second loads the stored cubin without compiling; both encode
+    bit-exactly."""
+    import os
+    import subprocess
+    import sys
+    code = (
+        "import numpy as np, torch, oracle as O, reedsolomon_b200 as rs\n"
+        "k, p, S = 7, 3, 1 << 20\n"
+        "data = O.seeded_shards(4242, k, S); want = data + [np.zeros(S, np.uint8) for _ in range(p)]\n"
+        "O.rs_encode(k, p, want)\n"
+        "rs.force_variant(7)\n"
+        "sh = [torch.from_numpy(d).cuda() for d in data] + [torch.zeros(S, dtype=torch.uint8, device='cuda') for _ in range(p)]\n"
+        "rs.New(k, p).Encode(sh)\n"
+        "assert all(np.array_equal(sh[i].cpu().numpy(), want[i]) for i in range(k, k + p))\n"
+        "print('files', len(__import__('os').listdir(__import__('os').environ['RSGPU_KERNEL_CACHE'])))\n")
+    env = dict(os.environ, RSGPU_KERNEL_CACHE=str(tmp_path / "kc"))
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env["PYTHONPATH"] = root + os.pathsep + env.get("PYTHONPATH", "")
+    outs, stamps = [], []
+    for _ in range(2):
+        r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr[-3000:]
+        outs.append(r.stdout.strip())
+        (f,) = list((tmp_path / "kc").iterdir())
+        stamps.append(f.stat().st_mtime_ns)
+    assert outs[0] == outs[1] == "files 1"
+    assert stamps[0] == stamps[1]   # the second process loaded the file, it did not rewrite it
