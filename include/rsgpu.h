@@ -360,6 +360,11 @@ int rsgpu_xornet_available(void);
 /* Waits for queued background compiles; returns how many XOR-network
  * kernels are compiled in this process. */
 int rsgpu_xornet_sync(void);
+/* Compiles now the XOR-network kernels a classic encoder's Encode and Verify
+ * launch (every input / output tile), so their first calls run the network
+ * rather than a table kernel.  Needs no device.  Returns the number of
+ * kernels ready (0 for Leopard encoders or without NVRTC). */
+int rsgpu_encoder_prepare_kernels(rsgpu_encoder *enc);
 /* Generated source for an n_out x n_in coefficient tile (row-major,
  * n_in <= 32, n_out <= 16) in one mode (0 write, 1 xor into the outputs,
  * 2 compare with them), factoring `group` inputs at a time (0: the default

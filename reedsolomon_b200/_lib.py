@@ -111,6 +111,7 @@ SIGNATURES = {
     "rsgpu_record_variant": (c_int, [c_int, c_int, c_size, c_int, c_int]),
     "rsgpu_xornet_available": (c_int, []),
     "rsgpu_xornet_sync": (c_int, []),
+    "rsgpu_encoder_prepare_kernels": (c_int, [c_voidp]),
     "rsgpu_xornet_source": (ctypes.c_longlong, [c_voidp, c_int, c_int, c_int, c_int, c_int, ctypes.c_char_p,
                                                 c_size]),
     "rsgpu_update": (c_int, [c_voidp, c_voidp, c_voidp, c_size]),

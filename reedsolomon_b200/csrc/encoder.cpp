@@ -904,6 +904,29 @@ int rsgpu_xornet_available(void) { return xornet_available() ? 1 : 0; }
 
 int rsgpu_xornet_sync(void) { return xornet_wait_idle(); }
 
+int rsgpu_encoder_prepare_kernels(rsgpu_encoder *enc) {
+    if (!enc) return RS_ERR_INVALID_INPUT;
+    if (enc->codec != RS_CODEC_CLASSIC || enc->p == 0 || !xornet_available()) return 0;
+    // The tiles launch_gf8_matmul runs for Encode (the first input tile
+    // writes, later ones XOR) and for Verify (up to 32 inputs: one compare).
+    int n = 0;
+    const int k = enc->k, p = enc->p;
+    const uint8_t *rows = enc->parity_rows.data();
+    const uint8_t *no_in[kMaxIn] = {};  // kernels depend on the coefficients only
+    uint8_t *no_out[kMaxOut] = {};
+    for (int o0 = 0; o0 < p; o0 += kMaxOut) {
+        const int no = std::min(kMaxOut, p - o0);
+        for (int i0 = 0; i0 < k; i0 += kMaxIn) {
+            const int ni = std::min(kMaxIn, k - i0);
+            GfMatArgs a;
+            fill_args(a, rows + (size_t)o0 * k + i0, k, ni, no, no_in, no_out, 0, nullptr);
+            n += xornet_prepare(a, i0 == 0 ? kModeWrite : kModeXor) ? 1 : 0;
+            if (k <= kMaxIn) n += xornet_prepare(a, kModeVerify) ? 1 : 0;
+        }
+    }
+    return n;
+}
+
 long long rsgpu_xornet_source(const uint8_t *coef, int n_in, int n_out, int mode, int group, int host,
                               char *buf, size_t cap) {
     if (!coef || n_in <= 0 || n_in > kMaxIn || n_out <= 0 || n_out > kXornetMaxOut || mode < 0 ||

@@ -207,6 +207,14 @@ class Encoder:
         except Exception:
             pass
 
+    def PrepareKernels(self):
+        """Compiles now the generated kernels this encoder's Encode and Verify
+        use (no device needed); returns how many are ready."""
+        n = L.lib().rsgpu_encoder_prepare_kernels(self._h)
+        if n < 0:
+            check(n)
+        return n
+
     # Extensions
     def DataShards(self):
         return self._k

@@ -196,3 +196,17 @@ def test_python_tuning_helpers_without_device():
     with pytest.raises(rs.RSError):
         rs.force_variant(99)
     assert rs.wait_generated_kernels() >= 0
+
+
+@pytest.mark.skipif(_nvrtc() is None, reason="libnvrtc.so.12 not loadable")
+def test_prepare_kernels_without_device():
+    """PrepareKernels compiles the Encode/Verify networks of a host-only
+    encoder: one write and one compare kernel for k <= 32; for k = 40,
+    p = 20 the write kernel of the first input tile and the xor kernels of
+    the second, for both output tiles (verify composes write kernels)."""
+    before = rs.wait_generated_kernels()
+    assert rs.New(10, 4, rs.HostOnly()).PrepareKernels() == 2
+    assert rs.New(40, 20, rs.HostOnly()).PrepareKernels() == 4
+    assert rs.New(10, 4, rs.HostOnly(), rs.WithLeopardGF16()).PrepareKernels() == 0
+    assert rs.wait_generated_kernels() >= before + 6
+    assert rs.New(10, 4, rs.HostOnly()).PrepareKernels() == 2   # cached: no new compile
