@@ -33,6 +33,7 @@
 #include <dlfcn.h>
 #include <nvrtc.h>
 
+#include <pthread.h>
 #include <sys/stat.h>
 #include <unistd.h>
 
@@ -48,6 +49,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <new>
 #include <string>
 #include <thread>
 #include <vector>
@@ -413,8 +415,48 @@ struct Cache {
     int busy = 0;
 };
 
+void worker_loop();
+Cache &cache();
+
+// Starts a compile worker when queued work has no free one, up to a quarter
+// of the host threads (1..4).  Workers never exit (the queue and the cache
+// outlive static teardown).  Called with the cache lock held.
+void spawn_workers_locked(Cache &c) {
+    const int cap = std::max(1, std::min(4, (int)std::thread::hardware_concurrency() / 4));
+    if (!c.queue.empty() && c.workers < cap && c.busy == c.workers) {
+        std::thread(worker_loop).detach();
+        c.workers++;
+    }
+}
+
+// fork(): the child inherits none of the worker threads.  The lock is held
+// across fork so the child's copy of the cache is consistent; the child then
+// forgets the workers, puts back in the queue the matrices that were being
+// compiled, and starts workers on demand (the next queued compile or wait),
+// not from the handler.  Condition variables are rebuilt: no thread waits
+// on them in the child.
+void fork_prepare() { cache().mu.lock(); }
+void fork_parent() { cache().mu.unlock(); }
+void fork_child() {
+    Cache &c = cache();
+    new (&c.cv) std::condition_variable();
+    new (&c.idle) std::condition_variable();
+    c.workers = 0;
+    c.busy = 0;
+    for (auto &kv : c.map)
+        if (kv.second->state == Entry::kCompiling) {
+            kv.second->state = Entry::kQueued;
+            c.queue.emplace_back(kv.first, kv.second);
+        }
+    c.mu.unlock();
+}
+
 Cache &cache() {
-    static Cache *c = new Cache();  // never destroyed (see nvrtc())
+    static Cache *c = [] {
+        Cache *p = new Cache();  // never destroyed (see nvrtc())
+        pthread_atfork(fork_prepare, fork_parent, fork_child);
+        return p;
+    }();
     return *c;
 }
 
@@ -587,13 +629,7 @@ std::shared_ptr<Entry> lookup(const GfMatArgs &a, int mode, bool sync) {
             c.map.emplace(key, e);
             if (!sync) {
                 c.queue.emplace_back(key, e);
-                // Up to a quarter of the host threads (1..4) compile; they
-                // never exit (the queue and cache outlive static teardown).
-                const int cap = std::max(1, std::min(4, (int)std::thread::hardware_concurrency() / 4));
-                if (c.workers < cap && c.busy == c.workers) {
-                    std::thread(worker_loop).detach();
-                    c.workers++;
-                }
+                spawn_workers_locked(c);
                 c.cv.notify_one();
                 return nullptr;
             }
@@ -631,6 +667,8 @@ bool xornet_prepare(const GfMatArgs &a, int mode) {
 int xornet_wait_idle() {
     Cache &c = cache();
     std::unique_lock<std::mutex> lk(c.mu);
+    spawn_workers_locked(c);  // queued work without workers (a forked child)
+    c.cv.notify_all();
     c.idle.wait(lk, [&] { return c.queue.empty() && c.busy == 0; });
     int n = 0;
     for (auto &kv : c.map) n += kv.second->state == Entry::kCompiled;

@@ -1,9 +1,9 @@
 """Concurrency of the XOR-network compile cache, on the CPU: background
 compiles queued through the launch path (which returns before any CUDA call
 while a matrix is not compiled) race synchronous compiles of the same and of
-new matrices.  The harness (tests/xornet_cache_stress.cpp) links the
-library's internal C++ entry points and must finish without deadlock, with
-every synchronous compile succeeding."""
+new matrices; and compiles queued before fork() finish in both processes.
+The harnesses (tests/xornet_cache_stress.cpp, tests/xornet_fork.cpp) link
+the library's internal C++ entry points and must finish without deadlock."""
 import ctypes
 import os
 import shutil
@@ -39,3 +39,23 @@ def test_sync_and_background_compiles_do_not_deadlock(tmp_path):
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "bad=0" in r.stdout
+
+
+@pytest.mark.skipif(shutil.which("g++") is None or not os.path.isdir(CUDA_INC) or not _nvrtc(),
+                    reason="needs g++, CUDA headers and libnvrtc")
+def test_queued_compiles_survive_fork(tmp_path):
+    rs.lib()
+    exe = tmp_path / "fork"
+    r = subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(PKG, "csrc"), "-I", os.path.join(ROOT, "include"),
+                        "-I", CUDA_INC, os.path.join(HERE, "xornet_fork.cpp"), "-o", str(exe),
+                        "-L", PKG, "-lrsgpu", "-Wl,-rpath," + PKG, "-lpthread"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
+    # own process group, so a hung child is killed with its parent
+    p = subprocess.Popen([str(exe)], stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True, start_new_session=True)
+    try:
+        out, err = p.communicate(timeout=300)
+    except subprocess.TimeoutExpired:
+        os.killpg(p.pid, 9)
+        raise
+    assert p.returncode == 0, out + err
+    assert "child ok=1" in out and "child_status=0" in out
