@@ -582,6 +582,7 @@ struct DrainAtExit {
         std::unique_lock<std::mutex> lk(c.mu);
         for (auto &q : c.queue) q.second->state = Entry::kFailed;
         c.queue.clear();
+        c.idle.notify_all();  // waiters for an empty queue
         c.idle.wait_for(lk, std::chrono::seconds(30), [&] { return c.busy == 0; });
     }
 } g_drain_at_exit;
