@@ -210,3 +210,37 @@ def test_prepare_kernels_without_device():
     assert rs.New(10, 4, rs.HostOnly(), rs.WithLeopardGF16()).PrepareKernels() == 0
     assert rs.wait_generated_kernels() >= before + 6
     assert rs.New(10, 4, rs.HostOnly()).PrepareKernels() == 2   # cached: no new compile
+
+
+def _network_xors(src):
+    body = src[src.index("for (; c < XN_N"):]
+    return sum(line.count("^") for line in body.split("\n")
+               if (line.startswith("o") and "^=" in line) or line.startswith("const u32 t"))
+
+
+def test_factoring_keeps_the_network_small():
+    """The generated RS(10,4) network needs 632 two-input XORs after pair
+    factoring, about half of the 1224 single-bit terms of its bit matrix; a
+    generator change that loses the factoring shows up here before it shows
+    up as a slower kernel."""
+    coef = reference_parity(10, 4)
+    terms = sum(bin(O.gal_mul(int(coef[j][i]), 1 << a)).count("1")
+                for j in range(4) for i in range(10) for a in range(8))
+    assert terms == 1224
+    assert _network_xors(source(coef, WRITE, 0)) <= 660
+
+
+@pytest.mark.skipif(_nvrtc() is None, reason="libnvrtc.so.12 not loadable")
+@pytest.mark.parametrize("ni,no,mode", [(1, 1, WRITE), (32, 1, VERIFY), (1, 16, XOR), (32, 16, VERIFY), (2, 7, WRITE)])
+def test_corner_tiles_compile(ni, no, mode):
+    """Extreme tile shapes, each in the group size the library tries first,
+    go through NVRTC for sm_100a."""
+    nv = _nvrtc()
+    coef = np.random.default_rng(ni * 17 + no).integers(0, 256, (no, ni), dtype=np.uint8)
+    src = source(coef, mode, 0).encode()
+    prog = ctypes.c_void_p()
+    assert nv.nvrtcCreateProgram(ctypes.byref(prog), src, b"rs_xornet.cu", 0, None, None) == 0
+    opts = [b"--gpu-architecture=sm_100a", b"--std=c++17", b"-default-device"]
+    rc = nv.nvrtcCompileProgram(prog, len(opts), (ctypes.c_char_p * len(opts))(*opts))
+    nv.nvrtcDestroyProgram(ctypes.byref(prog))
+    assert rc == 0
