@@ -195,3 +195,55 @@ def test_oracle_update_and_decode_idx_properties():
     assert O.rs_decode_idx(k, p, dst_a, expect, bad, S) == O.ERR["invalid_input"]
     few = [1, 1, 1] + [0] * (k + p - 3)
     assert O.rs_decode_idx(k, p, [None] * (k + p), few, [None] * (k + p), S) == O.ERR["too_few_shards"]
+
+
+@pytest.mark.parametrize("gf,k,p,size", [(16, 20, 13, 192), (16, 300, 60, 64), (8, 40, 24, 128), (8, 192, 56, 64)])
+def test_oracle_leopard_encode_is_linear(gf, k, p, size):
+    """Leopard output bytes have no golden vectors in the reference; these
+    are properties any correct encoder has: parity of zero data is zero,
+    parity(a ^ b) = parity(a) ^ parity(b), and parity(c * a) = c * parity(a)
+    symbol by symbol, with the product of Leopard's own field (its
+    Cantor-basis log/exp tables, leopard.go:1104-1147, leopard8.go:1018-1060),
+    not galMultiply."""
+    rng = np.random.default_rng(gf + k + p)
+
+    def parity(data):
+        sh = [d.copy() for d in data] + [np.zeros(size, np.uint8) for _ in range(p)]
+        assert O.leo_encode(gf, k, p, sh) == 0
+        return sh[k:]
+
+    a = [rng.integers(0, 256, size, dtype=np.uint8) for _ in range(k)]
+    b = [rng.integers(0, 256, size, dtype=np.uint8) for _ in range(k)]
+    assert all(not x.any() for x in parity([np.zeros(size, np.uint8) for _ in range(k)]))
+    pa, pb = parity(a), parity(b)
+    pab = parity([x ^ y for x, y in zip(a, b)])
+    assert all(np.array_equal(z, x ^ y) for z, x, y in zip(pab, pa, pb))
+    if gf == 8:
+        log, exp, _, _ = O.leo8_tables()
+        c = 0x53
+
+        def mul(v):  # mulLog8 with addMod8's partial reduction
+            if v == 0:
+                return 0
+            t = int(log[v]) + int(log[c])
+            return int(exp[(t + (t >> 8)) & 0xFF])
+
+        table = np.array([mul(v) for v in range(256)], np.uint8)
+        pc = parity([table[x] for x in a])
+        assert all(np.array_equal(z, table[x]) for z, x in zip(pc, pa))
+    else:
+        # GF(2^16): symbol j of each 64-byte chunk is byte j | byte 32+j << 8
+        # (leopard.go:907-925); scale every symbol by c with mulLog
+        log, exp, _, _ = O.leo16_tables()
+        c = 0x1D3A
+
+        def scale(shard):
+            ch = shard.reshape(-1, 64).astype(np.uint32)
+            sym = ch[:, :32] | (ch[:, 32:] << 8)
+            t = log[sym].astype(np.uint32) + int(log[c])
+            t = (t + (t >> 16)) & 0xFFFF
+            out = np.where(sym == 0, 0, exp[t].astype(np.uint32))
+            return np.concatenate([out & 0xFF, out >> 8], axis=1).astype(np.uint8).reshape(-1)
+
+        pc = parity([scale(x) for x in a])
+        assert all(np.array_equal(z, scale(x)) for z, x in zip(pc, pa))
