@@ -247,3 +247,25 @@ def test_oracle_leopard_encode_is_linear(gf, k, p, size):
 
         pc = parity([scale(x) for x in a])
         assert all(np.array_equal(z, scale(x)) for z, x in zip(pc, pa))
+
+
+@pytest.mark.parametrize("gf,k,p", [(16, 5, 3), (16, 7, 4), (8, 5, 3), (8, 6, 5)])
+def test_oracle_leopard_recovers_every_pattern(gf, k, p):
+    """Leopard is MDS: every set of up to p lost shards (data or parity) is
+    recovered exactly, and exactly the lost shards are written."""
+    import itertools
+    size = 64
+    rng = np.random.default_rng(100 * gf + k)
+    ref = [rng.integers(0, 256, size, dtype=np.uint8) for _ in range(k)] + [np.zeros(size, np.uint8) for _ in range(p)]
+    assert O.leo_encode(gf, k, p, ref) == 0
+    n = 0
+    for e in range(1, p + 1):
+        for lost in itertools.combinations(range(k + p), e):
+            sh = [np.zeros(size, np.uint8) if i in lost else ref[i].copy() for i in range(k + p)]
+            present = [0 if i in lost else 1 for i in range(k + p)]
+            rc, written = O.leo_reconstruct(gf, k, p, sh, present, recover_all=True)
+            assert rc == 0, lost
+            assert all(np.array_equal(a, b) for a, b in zip(sh, ref)), lost
+            assert sorted(i for i, w in enumerate(written) if w) == list(lost)
+            n += 1
+    assert n == sum(len(list(itertools.combinations(range(k + p), e))) for e in range(1, p + 1))
