@@ -218,3 +218,21 @@ def test_errloc_cache_repeats_and_overflow(gf):
                 assert np.array_equal(host(sh[i]), ref[i]), (rnd, lost, i)
         assert lib.rsgpu_leopard_errloc_cached(enc._h) == 256
     assert lib.rsgpu_leopard_errloc_cached(rs.New(4, 2)._h) == 0
+
+
+@pytest.mark.parametrize("gf,k,p", [(16, 5, 3), (16, 7, 4), (8, 5, 3)])
+def test_every_erasure_pattern_small_codes(gf, k, p):
+    """Every set of up to p lost shards of a small Leopard code is rebuilt
+    on the device byte for byte (the oracle recovers them all too)."""
+    import itertools
+    size = 128
+    rng = np.random.default_rng(700 + 10 * gf + k)
+    ref = [rng.integers(0, 256, size, dtype=np.uint8) for _ in range(k)] + [np.zeros(size, np.uint8) for _ in range(p)]
+    assert O.leo_encode(gf, k, p, ref) == 0
+    enc = new(gf, k, p)
+    for e in range(1, p + 1):
+        for lost in itertools.combinations(range(k + p), e):
+            sh = [None if i in lost else dev(ref[i]) for i in range(k + p)]
+            enc.Reconstruct(sh)
+            for i in lost:
+                assert np.array_equal(host(sh[i]), ref[i]), (lost, i)
