@@ -1,0 +1,272 @@
+// gf8_rt.cuh -- bit-sliced GF(2^8) contraction with run-time coefficients.
+//
+// Multiplication by a constant c in GF(2^8) is linear over GF(2): bit b of
+// c*x is the XOR of the bits a of x for which bit b of c*2^a is set (the 8x8
+// bit matrices of the reference's GFNI path, genGFNIMatrix, galois.go:
+// 1004-1016).  On bit-planes (bit a of 32 bytes in one 32-bit word) a product
+// is therefore a fixed XOR pattern of whole words, about 18 three-input LOP3s
+// for a random coefficient.  The run-time generated XOR network (xornet.cpp)
+// bakes one matrix's coefficients into straight-line code and needs an NVRTC
+// compile per matrix; this kernel is compiled once, ahead of time:
+//
+//   * all 256 "accumulate c*x" bodies exist in the binary, one per constant,
+//     each a straight line of LOP3s over eight plane registers;
+//   * the coefficient of (output j, input i) is read at run time (kernel
+//     parameter space, warp-uniform) and a switch jumps to its body: every
+//     lane of a warp takes the same branch, so there is no divergence, only
+//     the jump itself per (j, i) pair;
+//   * a warp owns 1 KiB of every shard per step (lane l holds 16-byte vectors
+//     l and l+32), transposes each input's eight words into bit-planes (three
+//     delta-swap stages), keeps 4 x 8 accumulator planes in registers per
+//     pass over the inputs, and transposes them back.
+//
+// Register arrays cannot be indexed by a run-time input number, and inlining
+// one 256-way switch per (output, input) pair makes the code, and ptxas's time
+// (quadratic in the copies), explode.  So a warp's inputs are staged raw in
+// a ring of 1 KiB slots in shared memory with cp.async: each lane owns its
+// own 16-byte slots (no synchronisation, no bank conflicts), the input loop
+// stays rolled, and the kernel holds exactly four switch copies (one per
+// accumulated output).  The next chunk's inputs are copied into the slots as
+// this chunk consumes them, so loads overlap the arithmetic.
+//
+// Any decode matrix (Reconstruct, ReconstructData, ReconstructSome, DecodeIdx)
+// therefore runs the bit-sliced path on first sight, with no compile and no
+// module load.
+#pragma once
+
+#include <cstdint>
+#include <type_traits>
+#include <utility>
+
+#include "kernels.h"
+
+namespace rsgpu {
+namespace gf8rt {
+
+constexpr int kChunk = 1024;  // bytes of every shard per warp step
+constexpr int kPass = 4;      // outputs accumulated in registers per pass over the inputs
+
+// GF(2^8) product, polynomial 0x11D (galois.go's field), at compile time.
+constexpr uint32_t cmul(uint32_t a, uint32_t b) {
+    uint32_t r = 0;
+    for (int i = 0; i < 8; i++) {
+        if (b & 1u) r ^= a;
+        b >>= 1;
+        a = (a << 1) ^ ((a & 0x80u) ? 0x11Du : 0u);
+    }
+    return r & 0xFFu;
+}
+
+// Bit (8b + a) set when plane a of x feeds plane b of c*x.
+constexpr uint64_t bitmat(uint32_t c) {
+    uint64_t m = 0;
+    for (int a = 0; a < 8; a++) {
+        const uint32_t col = cmul(c, 1u << a);
+        for (int b = 0; b < 8; b++)
+            if ((col >> b) & 1u) m |= 1ull << (8 * b + a);
+    }
+    return m;
+}
+
+// y ^= C * x on bit-planes.  Each row is one XOR chain that the compiler
+// fuses into three-input LOP3s.
+template <int C>
+__device__ __forceinline__ void mul_acc(uint32_t (&y)[8], const uint32_t (&x)[8]) {
+    constexpr uint64_t M = bitmat((uint32_t)C);
+#pragma unroll
+    for (int b = 0; b < 8; b++) {
+        uint32_t t = y[b];
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+            if ((M >> (8 * b + a)) & 1ull) t ^= x[a];
+        y[b] = t;
+    }
+}
+
+#define RSGPU_RT_CASE(n)  \
+    case n:               \
+        mul_acc<n>(y, x); \
+        break;
+#define RSGPU_RT_CASE16(h)                                                          \
+    RSGPU_RT_CASE(h * 16 + 0) RSGPU_RT_CASE(h * 16 + 1) RSGPU_RT_CASE(h * 16 + 2)   \
+    RSGPU_RT_CASE(h * 16 + 3) RSGPU_RT_CASE(h * 16 + 4) RSGPU_RT_CASE(h * 16 + 5)   \
+    RSGPU_RT_CASE(h * 16 + 6) RSGPU_RT_CASE(h * 16 + 7) RSGPU_RT_CASE(h * 16 + 8)   \
+    RSGPU_RT_CASE(h * 16 + 9) RSGPU_RT_CASE(h * 16 + 10) RSGPU_RT_CASE(h * 16 + 11) \
+    RSGPU_RT_CASE(h * 16 + 12) RSGPU_RT_CASE(h * 16 + 13) RSGPU_RT_CASE(h * 16 + 14) \
+    RSGPU_RT_CASE(h * 16 + 15)
+
+// y ^= c * x for a warp-uniform run-time coefficient c (c = 0: nothing).
+__device__ __forceinline__ void mul_acc_rt(uint32_t c, uint32_t (&y)[8], const uint32_t (&x)[8]) {
+    switch (c & 0xFFu) {
+        case 0:
+            break;
+        RSGPU_RT_CASE(1) RSGPU_RT_CASE(2) RSGPU_RT_CASE(3) RSGPU_RT_CASE(4) RSGPU_RT_CASE(5)
+        RSGPU_RT_CASE(6) RSGPU_RT_CASE(7) RSGPU_RT_CASE(8) RSGPU_RT_CASE(9) RSGPU_RT_CASE(10)
+        RSGPU_RT_CASE(11) RSGPU_RT_CASE(12) RSGPU_RT_CASE(13) RSGPU_RT_CASE(14) RSGPU_RT_CASE(15)
+        RSGPU_RT_CASE16(1) RSGPU_RT_CASE16(2) RSGPU_RT_CASE16(3) RSGPU_RT_CASE16(4) RSGPU_RT_CASE16(5)
+        RSGPU_RT_CASE16(6) RSGPU_RT_CASE16(7) RSGPU_RT_CASE16(8) RSGPU_RT_CASE16(9) RSGPU_RT_CASE16(10)
+        RSGPU_RT_CASE16(11) RSGPU_RT_CASE16(12) RSGPU_RT_CASE16(13) RSGPU_RT_CASE16(14) RSGPU_RT_CASE16(15)
+    }
+}
+
+// Exchanges bits (m << s) of x with bits m of y (one delta swap).
+__device__ __forceinline__ void dswap(uint32_t &x, uint32_t &y, uint32_t m, int s) {
+    const uint32_t xs = x >> s, ys = y << s;
+    x = (x & ~(m << s)) | (ys & (m << s));
+    y = (y & ~m) | (xs & m);
+}
+
+// 8x8 bit transpose of every byte lane of w[0..7] (an involution): word a
+// becomes bit-plane a of the 32 bytes the eight words hold.
+__device__ __forceinline__ void t8(uint32_t (&w)[8]) {
+    dswap(w[0], w[4], 0x0F0F0F0Fu, 4); dswap(w[1], w[5], 0x0F0F0F0Fu, 4);
+    dswap(w[2], w[6], 0x0F0F0F0Fu, 4); dswap(w[3], w[7], 0x0F0F0F0Fu, 4);
+    dswap(w[0], w[2], 0x33333333u, 2); dswap(w[1], w[3], 0x33333333u, 2);
+    dswap(w[4], w[6], 0x33333333u, 2); dswap(w[5], w[7], 0x33333333u, 2);
+    dswap(w[0], w[1], 0x55555555u, 1); dswap(w[2], w[3], 0x55555555u, 1);
+    dswap(w[4], w[5], 0x55555555u, 1); dswap(w[6], w[7], 0x55555555u, 1);
+}
+
+// Calls f(std::integral_constant<int, 0..N-1>) in order.  The loop bodies
+// below hold whole 256-way switches, far beyond what the compiler's loop
+// unroller accepts; unrolling them here keeps every register array indexed
+// by constants (a loop left rolled would move the arrays to local memory).
+template <typename F, int... Is>
+__device__ __forceinline__ void sfor_impl(F &&f, std::integer_sequence<int, Is...>) {
+    (f(std::integral_constant<int, Is>{}), ...);
+}
+template <int N, typename F>
+__device__ __forceinline__ void sfor(F &&f) {
+    sfor_impl(f, std::make_integer_sequence<int, N>{});
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t smem_addr, const void *gptr) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr), "l"(gptr) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+__device__ __forceinline__ void lds2(uint32_t sa, uint32_t (&x)[8]) {
+    asm volatile("ld.shared.v4.u32 {%0,%1,%2,%3}, [%4];" : "=r"(x[0]), "=r"(x[1]), "=r"(x[2]), "=r"(x[3]) : "r"(sa));
+    asm volatile("ld.shared.v4.u32 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(x[4]), "=r"(x[5]), "=r"(x[6]), "=r"(x[7])
+                 : "r"(sa + 512));
+}
+__device__ __forceinline__ void sts2(uint32_t sa, const uint32_t (&x)[8]) {
+    asm volatile("st.shared.v4.u32 [%0], {%1,%2,%3,%4};" ::"r"(sa), "r"(x[0]), "r"(x[1]), "r"(x[2]), "r"(x[3])
+                 : "memory");
+    asm volatile("st.shared.v4.u32 [%0], {%1,%2,%3,%4};" ::"r"(sa + 512), "r"(x[4]), "r"(x[5]), "r"(x[6]),
+                 "r"(x[7])
+                 : "memory");
+}
+
+// The result of one output (eight planes, transposed back here) goes to
+// 16-byte vectors v0 and v0+32 of dst: stored, XORed in, or compared.
+__device__ __forceinline__ void finish_output(uint32_t (&y)[8], uint4 *dst, long long v0, int mode, uint32_t &diff) {
+    t8(y);
+    const uint4 r0 = make_uint4(y[0], y[1], y[2], y[3]);
+    const uint4 r1 = make_uint4(y[4], y[5], y[6], y[7]);
+    if (mode == kModeWrite) {
+        __stcs(dst + v0, r0);
+        __stcs(dst + v0 + 32, r1);
+        return;
+    }
+    const uint4 e0 = __ldcs(dst + v0), e1 = __ldcs(dst + v0 + 32);
+    if (mode == kModeXor) {
+        __stcs(dst + v0, make_uint4(r0.x ^ e0.x, r0.y ^ e0.y, r0.z ^ e0.z, r0.w ^ e0.w));
+        __stcs(dst + v0 + 32, make_uint4(r1.x ^ e1.x, r1.y ^ e1.y, r1.z ^ e1.z, r1.w ^ e1.w));
+    } else {
+        diff |= (r0.x ^ e0.x) | (r0.y ^ e0.y) | (r0.z ^ e0.z) | (r0.w ^ e0.w) | (r1.x ^ e1.x) | (r1.y ^ e1.y) |
+                (r1.z ^ e1.z) | (r1.w ^ e1.w);
+    }
+}
+
+// One warp's step over chunk c (1 KiB of every shard) whose raw input vectors
+// have landed in the warp's ring (slot of input i: (base + i) mod ring).
+// Outputs are produced kPass at a time; with more than one pass the first
+// writes the transposed planes back into the ring so later passes skip the
+// transpose.  During the last pass, once input i's slot has been consumed,
+// issue_next(i + ahead, slot address) refills it with the next chunk's input.
+template <typename CoefFn, typename OutFn, typename NextFn>
+__device__ __forceinline__ void bitslice_step(uint32_t ring_s, int base, int ring, int lane, int n_in, int n_out,
+                                              int ahead, int mode, long long v0, CoefFn coef, OutFn out,
+                                              NextFn issue_next, uint32_t &diff) {
+    const int npass = (n_out + kPass - 1) / kPass;
+    for (int pass = 0; pass < npass; pass++) {
+        const bool last = pass + 1 == npass;
+        const int j0 = pass * kPass;
+        uint32_t y[kPass][8];
+        sfor<kPass>([&](auto J) { sfor<8>([&](auto B) { y[J][B] = 0; }); });
+        int slot = base;
+        for (int i = 0; i < n_in; i++) {
+            const uint32_t sa = ring_s + (uint32_t)(slot * kChunk + lane * 16);
+            uint32_t x[8];
+            lds2(sa, x);
+            if (pass == 0) {
+                t8(x);
+                if (!last) sts2(sa, x);
+            }
+            sfor<kPass>([&](auto J) {
+                if (j0 + J < n_out) mul_acc_rt(coef(j0 + J, i), y[J], x);
+            });
+            // x has been consumed (the products depend on it), so the slot
+            // may be overwritten by the next chunk's copy.
+            if (last && i + ahead < n_in) issue_next(i + ahead, sa);
+            slot = slot + 1 == ring ? 0 : slot + 1;
+        }
+        sfor<kPass>([&](auto J) {
+            if (j0 + J < n_out) finish_output(y[J], out(j0 + J), v0, mode, diff);
+        });
+    }
+}
+
+// out[j] (^)= sum_i coef[j][i] * in[i] over the first nchunk KiB of every
+// shard (16-byte aligned pointers), n_in <= 32 and n_out <= 16.  Each warp
+// owns a ring of n_in + ahead 1 KiB slots of dynamic shared memory.
+__global__ void __launch_bounds__(512, 1) gf8_bitslice_kernel(const __grid_constant__ GfMatArgs a, long long nchunk,
+                                                               int mode, int ahead) {
+    extern __shared__ __align__(16) uint8_t rt_smem[];
+    const int lane = threadIdx.x & 31;
+    const int n_in = a.n_in, n_out = a.n_out;
+    const int ring = n_in + ahead;
+    const uint32_t ring_s =
+        (uint32_t)__cvta_generic_to_shared(rt_smem) + (uint32_t)((threadIdx.x >> 5) * ring * kChunk);
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    auto issue = [&](long long chunk, int i, uint32_t sa) {
+        const uint4 *p = reinterpret_cast<const uint4 *>(a.in[i]) + chunk * 64 + lane;
+        cp_async16(sa, p);
+        cp_async16(sa + 512, p + 32);
+    };
+    int base = 0;
+    if (c < nchunk)
+        for (int i = 0; i < n_in; i++) issue(c, i, ring_s + (uint32_t)(i * kChunk + lane * 16));
+    uint32_t diff = 0;
+    for (; c < nchunk; c += nwarps) {
+        cp_async_wait_all();  // everything in flight belongs to chunk c
+        const long long cn = c + nwarps;
+        const bool has_next = cn < nchunk;
+        int nb = base + n_in;  // the next chunk's slot of input 0
+        if (nb >= ring) nb -= ring;
+        if (has_next) {  // its first `ahead` inputs go to the free slots now
+            int s = nb;
+            for (int i = 0; i < ahead; i++) {
+                issue(cn, i, ring_s + (uint32_t)(s * kChunk + lane * 16));
+                s = s + 1 == ring ? 0 : s + 1;
+            }
+        }
+        bitslice_step(
+            ring_s, base, ring, lane, n_in, n_out, ahead, mode, c * 64 + lane,
+            [&](int j, int i) -> uint32_t { return a.coef[j][i]; },
+            [&](int j) { return reinterpret_cast<uint4 *>(a.out[j]); },
+            [&](int i, uint32_t sa) {
+                if (has_next) issue(cn, i, sa);
+            },
+            diff);
+        base = nb;
+    }
+    cp_async_wait_all();
+    if (mode == kModeVerify && diff) *reinterpret_cast<volatile int *>(a.flag) = 1;
+}
+
+}  // namespace gf8rt
+}  // namespace rsgpu

@@ -44,7 +44,8 @@ enum GfVariant : int {
     kVariantFixed3 = 5, // as kVariantFixed, registers capped for 3 resident CTAs per SM
     kVariantFixed4 = 6, // as kVariantFixed, registers capped for 4 resident CTAs per SM
     kVariantXorNet = 7, // bit-sliced XOR network generated for the tile's coefficients (xornet.cpp)
-    kNumVariants = 8,
+    kVariantBitslice = 8, // bit-sliced, coefficients read at run time (gf8_rt.cuh): no compile per matrix
+    kNumVariants = 9,
 };
 
 // Force a variant for every launch (-1 restores the tuned / default choice).
@@ -68,6 +69,13 @@ cudaError_t launch_gf8_tile(cudaStream_t st, const DeviceInfo &dev, const GfMatA
 cudaError_t launch_gf8_matmul(cudaStream_t st, const DeviceInfo &dev, const uint8_t *rows, int n_in,
                               int n_out, const uint8_t *const *in, uint8_t *const *out,
                               size_t nbytes, int mode, int *d_flag, bool allow_generated = true);
+
+// Runs the bit-sliced run-time-coefficient kernel (kernels_gf8_bitslice.cu)
+// over the whole 1 KiB chunks of a (16-byte aligned shards, n_in <= 32,
+// n_out <= 16); *bytes_done is 0 when it did not run (unaligned pointers or
+// no whole chunk); the caller covers the rest.
+cudaError_t launch_bitslice(cudaStream_t st, const DeviceInfo &dev, const GfMatArgs &a, int mode,
+                            long long *bytes_done);
 
 // Fill an 8-byte aligned buffer with uniform pseudo-random bytes (tuning inputs).
 cudaError_t launch_fill_random(cudaStream_t st, const DeviceInfo &dev, uint8_t *p, size_t nbytes,

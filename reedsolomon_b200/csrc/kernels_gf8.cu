@@ -273,15 +273,16 @@ int choose_variant(int n_in, int n_out, int mode, size_t nbytes) {
     if (g_forced >= 0) return g_forced;
     auto it = g_tuned.find(std::make_tuple(n_in, (n_out + 3) / 4, mode, size_bucket(nbytes)));
     if (it != g_tuned.end()) return it->second;
-    // Untuned default: the generated XOR network from 256 KiB per shard when
+    // Untuned default from 256 KiB per shard: the generated XOR network when
     // NVRTC is present (faster than every table kernel at 16 MiB and above in
-    // all measured geometries, and at 1 MiB with enough SMs covered; the
-    // first launches of a new matrix run a table kernel while it compiles).
-    // Otherwise the unrolled table kernel with the most resident warps that
-    // does not spill (up to 4 outputs: 4 CTAs per SM when writing, 3 when the
-    // outputs are also read, which holds them in registers; 2 for 5-8
-    // outputs); input counts without a specialisation fall back to kVariantPrmt.
-    if (nbytes >= kXornetDefaultMin && xornet_available()) return kVariantXorNet;
+    // all measured geometries, and at 1 MiB with enough SMs covered); while a
+    // new matrix's network compiles, and without NVRTC, the bit-sliced kernel
+    // with run-time coefficients runs instead.  Below that size the unrolled
+    // table kernel with the most resident warps that does not spill (up to 4
+    // outputs: 4 CTAs per SM when writing, 3 when the outputs are also read,
+    // which holds them in registers; 2 for 5-8 outputs); input counts without
+    // a specialisation fall back to kVariantPrmt.
+    if (nbytes >= kXornetDefaultMin) return xornet_available() ? kVariantXorNet : kVariantBitslice;
     return table_variant(n_out, mode);
 }
 
@@ -316,13 +317,18 @@ cudaError_t launch_gf8_tile(cudaStream_t st, const DeviceInfo &dev, const GfMatA
     for (int i = 0; i < a.n_in; i++) vec_ok &= aligned16(a.in[i]);
     for (int o = 0; o < a.n_out; o++) vec_ok &= aligned16(a.out[o]);
     long long done = 0;
-    if (variant == kVariantXorNet) {
-        // Whole 1 KiB chunks through the generated kernel (compiled on the
-        // spot when forced, else in the background); the tail, or everything
-        // while the kernel is not ready, through the default table kernel.
-        cudaError_t e = xornet_launch(st, dev, a, mode, forced_variant() == kVariantXorNet, &done);
+    if (variant == kVariantXorNet || variant == kVariantBitslice) {
+        // Whole 1 KiB chunks through the generated network (compiled on the
+        // spot when forced, else in the background) or, when that is not
+        // ready or not asked for, through the bit-sliced run-time-coefficient
+        // kernel; the tail through the default table kernel.
+        cudaError_t e = cudaSuccess;
+        if (variant == kVariantXorNet)
+            e = xornet_launch(st, dev, a, mode, forced_variant() == kVariantXorNet, &done);
         if (e != cudaSuccess) return e;
-        variant = (a.n_out > 4) ? kVariantFixed2 : (mode == kModeWrite ? kVariantFixed4 : kVariantFixed3);
+        if (done == 0) e = launch_bitslice(st, dev, a, mode, &done);
+        if (e != cudaSuccess) return e;
+        variant = table_variant(a.n_out, mode);
         if (done == a.nbytes) return cudaGetLastError();
         if (done > 0) {
             GfMatArgs t = a;

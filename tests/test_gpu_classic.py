@@ -322,7 +322,7 @@ def test_shards_past_2gib_offsets():
     torch.cuda.empty_cache()
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8])
 def test_every_kernel_variant_bit_exact(variant):
     """Each variant of the GF(2^8) kernel (nibble-table address forms and the
     generated XOR network) gives the oracle's bytes."""
