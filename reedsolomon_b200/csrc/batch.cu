@@ -10,6 +10,7 @@
 // is 1/grid of the total, so consecutive tiles mostly share a job and its
 // shared-memory product tables, and the SMs finish together.
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <cstring>
 #include <map>
@@ -253,12 +254,16 @@ void plan_tiles(rsgpu_batch *b, std::vector<long long> &cta_first) {
         b->bytes += job_cost[i];
     }
     b->n_tiles = t;
-    static int resident = 0;
+    // resident CTAs per SM of the batch kernel, queried once per device
+    static std::atomic<int> resident_by_dev[64];
+    const int dev = b->ctx->info.device & 63;
+    int resident = resident_by_dev[dev].load(std::memory_order_relaxed);
     if (resident == 0) {
         const size_t smem = (size_t)kMaxIn * kInStride + kTableAlign;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, (const void *)gf8_batch_kernel, kThreads,
                                                           smem) != cudaSuccess || resident < 1)
             resident = 1;
+        resident_by_dev[dev].store(resident, std::memory_order_relaxed);
     }
     const int per_sm = std::min(resident, kBatchBlocksPerSm);
     const int grid = std::max(1, (int)std::min<long long>(t, (long long)b->ctx->info.sm_count * per_sm));

@@ -469,24 +469,31 @@ constexpr int kSpillOk = 128;
 // RSGPU_KERNEL_CACHE=<directory> keeps every final cubin in a file named by a
 // 64-bit FNV-1a hash of the kernel's generated source (preferred group), the
 // NVRTC version and the target, so a new process loads it instead of
-// compiling.  A file is used only when its header (magic, hash, size)
-// matches; files are written to a temporary name and renamed into place.
+// compiling.  A file is used only when its header (magic, source hash, size)
+// matches and the cubin bytes hash to the value stored beside them, so a
+// truncated or bit-flipped file is recompiled rather than run.  The hash is
+// a corruption check, not an authentication: whoever can write the directory
+// can make this process run their code, so it must be a directory only the
+// library's user can write (it is created with mode 0700).  Files are
+// written to a temporary name and renamed into place.
 struct DiskHeader {
     char magic[8];
-    uint64_t hash;
-    uint64_t size;
+    uint64_t hash;       // of the generated source, NVRTC version and target
+    uint64_t size;       // cubin bytes that follow
+    uint64_t body_hash;  // of those bytes
 };
-constexpr char kDiskMagic[8] = {'R', 'S', 'X', 'N', 'C', '0', '1', '\0'};
+constexpr char kDiskMagic[8] = {'R', 'S', 'X', 'N', 'C', '0', '2', '\0'};
 constexpr uint64_t kDiskMaxBytes = 64ull << 20;
 
-uint64_t fnv1a(const std::string &s) {
+uint64_t fnv1a(const char *p, size_t n) {
     uint64_t h = 0xcbf29ce484222325ull;
-    for (unsigned char c : s) {
-        h ^= c;
+    for (size_t i = 0; i < n; i++) {
+        h ^= (unsigned char)p[i];
         h *= 0x100000001b3ull;
     }
     return h;
 }
+uint64_t fnv1a(const std::string &s) { return fnv1a(s.data(), s.size()); }
 
 bool disk_read(const std::string &path, uint64_t hash, std::vector<char> &out) {
     FILE *f = fopen(path.c_str(), "rb");
@@ -496,7 +503,8 @@ bool disk_read(const std::string &path, uint64_t hash, std::vector<char> &out) {
               h.hash == hash && h.size > 0 && h.size <= kDiskMaxBytes;
     if (ok) {
         out.resize(h.size);
-        ok = fread(out.data(), 1, h.size, f) == h.size && fgetc(f) == EOF;
+        ok = fread(out.data(), 1, h.size, f) == h.size && fgetc(f) == EOF &&
+             fnv1a(out.data(), out.size()) == h.body_hash;
     }
     fclose(f);
     if (!ok) out.clear();
@@ -505,7 +513,7 @@ bool disk_read(const std::string &path, uint64_t hash, std::vector<char> &out) {
 
 void disk_write(const std::string &dir, const std::string &path, uint64_t hash, const std::vector<char> &bin) {
     static std::atomic<unsigned> seq{0};
-    mkdir(dir.c_str(), 0755);  // one level; an existing directory is fine
+    mkdir(dir.c_str(), 0700);  // one level; an existing directory is used as it is
     const std::string tmp = path + ".tmp." + std::to_string((long)getpid()) + "." + std::to_string(seq++);
     FILE *f = fopen(tmp.c_str(), "wb");
     if (!f) return;
@@ -513,6 +521,7 @@ void disk_write(const std::string &dir, const std::string &path, uint64_t hash, 
     memcpy(h.magic, kDiskMagic, sizeof kDiskMagic);
     h.hash = hash;
     h.size = bin.size();
+    h.body_hash = fnv1a(bin.data(), bin.size());
     const bool ok = fwrite(&h, sizeof h, 1, f) == 1 && fwrite(bin.data(), 1, bin.size(), f) == bin.size();
     if (fclose(f) == 0 && ok) rename(tmp.c_str(), path.c_str());
     else remove(tmp.c_str());

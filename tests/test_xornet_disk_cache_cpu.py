@@ -75,7 +75,19 @@ def test_damaged_file_is_recompiled(harness, tmp_path):
     victim.write_bytes(data + b"x")                      # trailing garbage
     n, ok = run(harness, d)
     assert ok == 3 and n >= 1
+    flipped = bytearray(data)
+    flipped[-100] ^= 0x04                                # a bit flipped inside the cubin
+    victim.write_bytes(bytes(flipped))
+    n, ok = run(harness, d)
+    assert ok == 3 and n >= 1
+    assert victim.read_bytes() == data
     assert run(harness, d) == (0, 3)
+
+
+def test_cache_directory_is_private(harness, tmp_path):
+    d = tmp_path / "kernels"
+    run(harness, d)
+    assert (os.stat(d).st_mode & 0o777) == 0o700
 
 
 def test_no_cache_without_the_variable(harness, tmp_path):
