@@ -73,3 +73,31 @@ def test_single_rank_max_is_identity():
     sys.path.insert(0, ROOT)
     import bench
     assert bench.max_over_ranks(3.25, 1, "cpu") == 3.25
+
+
+def test_bench_spawns_its_ranks_without_a_launcher():
+    """`bench.py --gpus 2` started without torchrun starts two ranks itself;
+    the reference arm prints one line, from rank 0, naming both GPUs' worth
+    of ranks and the same config as the product arm."""
+    import json
+    import subprocess
+    env = dict(os.environ)
+    for v in ("WORLD_SIZE", "RANK", "LOCAL_RANK", "MASTER_ADDR", "MASTER_PORT"):
+        env.pop(v, None)
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2",
+                        "--steps", "1", "--warmup", "0"], env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(l) for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    sys.path.insert(0, ROOT)
+    import bench
+    assert lines[0]["impl"] == "reference" and lines[0]["n_gpus"] == 2
+    assert lines[0]["config"] == bench.workload_config(2)
+
+
+def test_bench_refuses_a_rank_count_mismatch():
+    import subprocess
+    env = dict(os.environ, WORLD_SIZE="1", RANK="0", LOCAL_RANK="0")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2"],
+                       env=env, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 2 and "must match" in r.stderr
