@@ -180,6 +180,21 @@ int rsgpu_reconstruct_async(rsgpu_encoder *enc, uint8_t *const *shards, const ui
 int rsgpu_encode_host(rsgpu_encoder *enc, uint8_t *const *host_shards, size_t shard_size);
 int rsgpu_reconstruct_host(rsgpu_encoder *enc, uint8_t **host_shards, const uint8_t *present,
                            size_t shard_size, int data_only, uint8_t *written);
+/* ReconstructSome (reedsolomon.go:1655; leopard.go:386-391) on host buffers. */
+int rsgpu_reconstruct_some_host(rsgpu_encoder *enc, uint8_t **host_shards, const uint8_t *present,
+                                const uint8_t *required, int n_required, size_t shard_size, uint8_t *written);
+/* Verify (reedsolomon.go:857-871; leopard.go:393-419) on host buffers: every
+ * shard goes H2D, only the outcome comes back. */
+int rsgpu_verify_host(rsgpu_encoder *enc, uint8_t *const *host_shards, size_t shard_size, int *ok);
+/* EncodeIdx (reedsolomon.go:708-757) on host buffers: parity[o] ^= M[k+o][idx] * data. */
+int rsgpu_encode_idx_host(rsgpu_encoder *enc, const uint8_t *host_data, int idx, uint8_t *const *host_parity,
+                          size_t shard_size);
+/* Update (reedsolomon.go:762-853) on host buffers, with rsgpu_update's semantics. */
+int rsgpu_update_host(rsgpu_encoder *enc, uint8_t *const *host_shards, const uint8_t *const *host_new_data,
+                      size_t shard_size);
+/* DecodeIdx (reedsolomon.go:1464-1617) on host buffers, with rsgpu_decode_idx's semantics. */
+int rsgpu_decode_idx_host(rsgpu_encoder *enc, uint8_t *const *host_dst, const uint8_t *expect,
+                          const uint8_t *const *host_input, size_t shard_size);
 
 /* Decode planning without device work: the rows codeSomeShards receives in
  * reconstruct (reedsolomon.go:1710-1779).  rows_out[n_out x k], out_idx[n_out],
@@ -204,12 +219,14 @@ int rsgpu_check_some_shards(rsgpu_ctx *ctx, const uint8_t *rows, int n_in, int n
  * context, no allocation.  Its scratch is one 8 MiB array per device, static in
  * the library and held until exit; more than 32 inputs need
  * n_out * round_up(nbytes, 256) <= 8 MiB - 256, larger calls return
- * RS_ERR_INVALID_INPUT.  Only the table kernels run (the run-time compiled
- * XOR-network kernels load a module, which allocates device memory).  Runs
- * on `cuda_stream` on the current device and waits for it.  The first call
- * on a device looks up the array's device address; make it before any
- * stream capture.  Calls that overlap on the GPU share the array and race:
- * serialise them. */
+ * RS_ERR_INVALID_INPUT.  It runs one fixed set of table kernels (never the
+ * run-time compiled ones).  Runs on `cuda_stream` on the current device and
+ * waits for it.  The first call on a device does the set-up that does take
+ * memory: it looks up the array's device address and loads the array and
+ * every kernel the calls use (CUDA loads code lazily, on first use, and
+ * loading allocates); later calls on that device allocate nothing.  Make
+ * that first call at start-up, before any stream capture.  Calls that
+ * overlap on the GPU share the array and race: serialise them. */
 int rsgpu_check_some_shards_noalloc(const uint8_t *rows, int n_in, int n_out,
                                     const uint8_t *const *in, const uint8_t *const *to_check,
                                     size_t nbytes, void *cuda_stream, int *ok);

@@ -98,6 +98,11 @@ SIGNATURES = {
     "rsgpu_reconstruct_async": (c_int, [c_voidp, c_voidp, c_voidp, c_size, c_int]),
     "rsgpu_encode_host": (c_int, [c_voidp, c_voidp, c_size]),
     "rsgpu_reconstruct_host": (c_int, [c_voidp, c_voidp, c_voidp, c_size, c_int, c_voidp]),
+    "rsgpu_reconstruct_some_host": (c_int, [c_voidp, c_voidp, c_voidp, c_voidp, c_int, c_size, c_voidp]),
+    "rsgpu_verify_host": (c_int, [c_voidp, c_voidp, c_size, c_intp]),
+    "rsgpu_encode_idx_host": (c_int, [c_voidp, c_voidp, c_int, c_voidp, c_size]),
+    "rsgpu_update_host": (c_int, [c_voidp, c_voidp, c_voidp, c_size]),
+    "rsgpu_decode_idx_host": (c_int, [c_voidp, c_voidp, c_voidp, c_voidp, c_size]),
     "rsgpu_decode_plan": (c_int, [c_voidp, c_voidp, c_int, c_voidp, c_int, c_voidp, c_voidp, c_intp, c_voidp]),
     "rsgpu_code_some_shards": (c_int, [c_voidp, c_voidp, c_int, c_int, c_voidp, c_voidp, c_size, c_size, c_int]),
     "rsgpu_check_some_shards": (c_int, [c_voidp, c_voidp, c_int, c_int, c_voidp, c_voidp, c_size, c_intp]),

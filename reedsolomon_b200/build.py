@@ -19,18 +19,26 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "librsgpu.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
+GEN = os.path.join(BUILD, "gen")  # generated headers (gen_rt_dispatch.py)
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "-I", INCLUDE, "-I", CSRC]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "-I", INCLUDE, "-I", CSRC, "-I", GEN]
 
 
 def _sources():
     return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cpp")))
 
 
+def _generate():
+    """Writes the generated headers (rewritten only when their text changes)."""
+    from reedsolomon_b200 import gen_rt_dispatch
+    gen_rt_dispatch.write(os.path.join(GEN, "gf8_rt_dispatch.inc"))
+
+
 def _headers_mtime():
     hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    hs += [os.path.join(GEN, f) for f in os.listdir(GEN) if f.endswith(".inc")]
     hs += [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE) if f.endswith(".h")]
     return max(os.path.getmtime(h) for h in hs) if hs else 0.0
 
@@ -49,6 +57,7 @@ def _compile(src, obj, ptxas_v):
 
 def build(force=False, ptxas_v=False, verbose=False):
     os.makedirs(BUILD, exist_ok=True)
+    _generate()
     hdr = _headers_mtime()
     jobs = []
     objs = []

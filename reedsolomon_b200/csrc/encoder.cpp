@@ -159,6 +159,66 @@ int classic_decode_plan(rsgpu_encoder *enc, const uint8_t *present, int data_onl
     return RS_OK;
 }
 
+// DecodeIdx planning (reedsolomon.go:1464-1617) from which shards arrive in
+// this call (has_in) and which are accumulated into (has_dst): the decode
+// matrix is the inverse of the first k expected rows (getDecodeMatrix,
+// :634-673, cached in the inversion tree under the unexpected set); parity
+// outputs take the parity row times that inverse.  rows is n_out x n_in over
+// the arriving inputs among the first k expected shards (others carry zero
+// coefficients and are skipped); in_shards / out_shards name them.
+int decode_idx_plan(rsgpu_encoder *enc, const uint8_t *expect, const uint8_t *has_in, const uint8_t *has_dst,
+                    std::vector<uint8_t> &rows, std::vector<int> &in_shards, std::vector<int> &out_shards) {
+    const int k = enc->k, total = enc->total;
+    rows.clear();
+    in_shards.clear();
+    out_shards.clear();
+    for (int i = 0; i < total; i++) {
+        if (has_in[i] && !expect[i]) return RS_ERR_INVALID_INPUT;  // unexpected input
+        if (expect[i] && has_dst[i]) return RS_ERR_INVALID_INPUT;  // dst of an expected input
+    }
+    std::vector<int> valid, invalid;
+    for (int i = 0; i < total; i++) (expect[i] ? valid : invalid).push_back(i);
+    if ((int)valid.size() < k) return RS_ERR_TOO_FEW_SHARDS;
+    std::shared_ptr<const Matrix> dec;
+    if (enc->tree) dec = enc->tree->get(invalid);
+    if (!dec) {
+        Matrix sub(k, k);
+        for (int r = 0; r < k; r++)
+            for (int c = 0; c < k; c++) sub.at(r, c) = enc->m.at(valid[r], c);
+        auto inv = std::make_shared<Matrix>();
+        int rc = mat_invert(sub, *inv);
+        if (rc) return rc;
+        dec = inv;
+        if (enc->tree) enc->tree->insert(invalid, inv);
+    }
+    std::vector<int> cols;
+    for (int col = 0; col < k; col++)
+        if (has_in[valid[col]]) cols.push_back(col);
+    for (int d = 0; d < total; d++)
+        if (has_dst[d]) out_shards.push_back(d);
+    if (cols.empty() || out_shards.empty()) return RS_OK;
+    const Gf256 &g = Gf256::get();
+    const int n_in = (int)cols.size(), n_out = (int)out_shards.size();
+    rows.resize((size_t)n_out * n_in);
+    std::vector<uint8_t> full(k);
+    for (int o = 0; o < n_out; o++) {
+        const int d = out_shards[o];
+        if (d < k) {
+            for (int c = 0; c < k; c++) full[c] = dec->at(d, c);
+        } else {
+            const uint8_t *pr = enc->m.row(d);
+            for (int c = 0; c < k; c++) {
+                uint8_t v = 0;
+                for (int t = 0; t < k; t++) v ^= g.mul[pr[t]][dec->at(t, c)];
+                full[c] = v;
+            }
+        }
+        for (int j = 0; j < n_in; j++) rows[(size_t)o * n_in + j] = full[cols[j]];
+    }
+    for (int j = 0; j < n_in; j++) in_shards.push_back(valid[cols[j]]);
+    return RS_OK;
+}
+
 static int classic_reconstruct(rsgpu_encoder *enc, uint8_t **shards, const uint8_t *present,
                                size_t size, int data_only, const uint8_t *required, int n_required,
                                uint8_t *written) {
@@ -640,7 +700,7 @@ int rsgpu_decode_idx(rsgpu_encoder *enc, uint8_t *const *dst, const uint8_t *exp
     if (enc->codec != RS_CODEC_CLASSIC) return RS_ERR_NOT_SUPPORTED;  // leopard.go:94, leopard8.go:90
     if (!dst || !input) return RS_ERR_INVALID_INPUT;
     std::lock_guard<std::recursive_mutex> lk(enc->ctx->mu);
-    const int k = enc->k, total = enc->total;
+    const int total = enc->total;
     if (!expect) {  // merging mode: dst[i] ^= input[i]
         for (int i = 0; i < total; i++)
             if (input[i] && !dst[i]) return RS_ERR_INVALID_INPUT;
@@ -649,63 +709,24 @@ int rsgpu_decode_idx(rsgpu_encoder *enc, uint8_t *const *dst, const uint8_t *exp
             if (input[i]) RS_CUDA(launch_xor(enc->ctx->stream, enc->ctx->info, input[i], dst[i], size));
         return sync(enc->ctx);
     }
+    std::vector<uint8_t> has_in(total), has_dst(total);
     for (int i = 0; i < total; i++) {
-        if (input[i] && !expect[i]) return RS_ERR_INVALID_INPUT;  // unexpected input
-        if (expect[i] && dst[i]) return RS_ERR_INVALID_INPUT;     // dst of an expected input
+        has_in[i] = input[i] != nullptr;
+        has_dst[i] = dst[i] != nullptr;
     }
-    std::vector<int> valid, invalid;
-    for (int i = 0; i < total; i++) (expect[i] ? valid : invalid).push_back(i);
-    if ((int)valid.size() < k) return RS_ERR_TOO_FEW_SHARDS;
-    // getDecodeMatrix (reedsolomon.go:634-673): inverse of the first k
-    // expected rows, cached in the inversion tree under the unexpected set.
-    std::shared_ptr<const Matrix> dec;
-    if (enc->tree) dec = enc->tree->get(invalid);
-    if (!dec) {
-        Matrix sub(k, k);
-        for (int r = 0; r < k; r++)
-            for (int c = 0; c < k; c++) sub.at(r, c) = enc->m.at(valid[r], c);
-        auto inv = std::make_shared<Matrix>();
-        int rc = mat_invert(sub, *inv);
-        if (rc) return rc;
-        dec = inv;
-        if (enc->tree) enc->tree->insert(invalid, inv);
-    }
-    // inputs present in this call; columns past the first k expected shards
-    // carry zero coefficients and are skipped
-    std::vector<int> cols;
-    for (int col = 0; col < k; col++)
-        if (input[valid[col]]) cols.push_back(col);
-    std::vector<int> outs;
-    for (int d = 0; d < total; d++)
-        if (dst[d]) outs.push_back(d);
-    if (cols.empty() || outs.empty() || size == 0) return RS_OK;
-    const Gf256 &g = Gf256::get();
-    const int n_in = (int)cols.size(), n_out = (int)outs.size();
-    std::vector<uint8_t> rows((size_t)n_out * n_in);
-    std::vector<uint8_t> full(k);
-    for (int o = 0; o < n_out; o++) {
-        const int d = outs[o];
-        if (d < k) {
-            for (int c = 0; c < k; c++) full[c] = dec->at(d, c);
-        } else {
-            const uint8_t *pr = enc->m.row(d);
-            for (int c = 0; c < k; c++) {
-                uint8_t v = 0;
-                for (int t = 0; t < k; t++) v ^= g.mul[pr[t]][dec->at(t, c)];
-                full[c] = v;
-            }
-        }
-        for (int j = 0; j < n_in; j++) rows[(size_t)o * n_in + j] = full[cols[j]];
-    }
-    std::vector<const uint8_t *> ins(n_in);
-    std::vector<uint8_t *> dsts(n_out);
-    for (int j = 0; j < n_in; j++) ins[j] = input[valid[cols[j]]];
-    for (int o = 0; o < n_out; o++) dsts[o] = dst[outs[o]];
-    int rc = run_matmul(enc->ctx, rows.data(), n_in, n_out, ins.data(), dsts.data(), size, kModeXor);
+    std::vector<uint8_t> rows;
+    std::vector<int> ins, outs;
+    int rc = decode_idx_plan(enc, expect, has_in.data(), has_dst.data(), rows, ins, outs);
+    if (rc || ins.empty() || outs.empty() || size == 0) return rc;
+    std::vector<const uint8_t *> in_ptrs;
+    std::vector<uint8_t *> dsts;
+    for (int i : ins) in_ptrs.push_back(input[i]);
+    for (int d : outs) dsts.push_back(dst[d]);
+    rc = run_matmul(enc->ctx, rows.data(), (int)ins.size(), (int)outs.size(), in_ptrs.data(), dsts.data(), size,
+                    kModeXor);
     if (rc) return rc;
     return sync(enc->ctx);
 }
-
 int rsgpu_verify(rsgpu_encoder *enc, uint8_t *const *shards, size_t size, int *ok) {
     RS_TRACE("rsgpu_verify");
     NEED_CTX(enc);

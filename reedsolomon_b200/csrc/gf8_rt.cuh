@@ -4,29 +4,30 @@
 // c*x is the XOR of the bits a of x for which bit b of c*2^a is set (the 8x8
 // bit matrices of the reference's GFNI path, genGFNIMatrix, galois.go:
 // 1004-1016).  On bit-planes (bit a of 32 bytes in one 32-bit word) a product
-// is therefore a fixed XOR pattern of whole words, about 18 three-input LOP3s
-// for a random coefficient.  The run-time generated XOR network (xornet.cpp)
+// is therefore a fixed XOR pattern of whole words.  The run-time generated XOR network (xornet.cpp)
 // bakes one matrix's coefficients into straight-line code and needs an NVRTC
 // compile per matrix; this kernel is compiled once, ahead of time:
 //
 //   * all 256 "accumulate c*x" bodies exist in the binary, one per constant,
-//     each a straight line of LOP3s over eight plane registers;
+//     each a straight line of at most eight LOP3s;
 //   * the coefficient of (output j, input i) is read at run time (kernel
-//     parameter space, warp-uniform) and a switch jumps to its body: every
-//     lane of a warp takes the same branch, so there is no divergence, only
-//     the jump itself per (j, i) pair;
+//     parameter space, warp-uniform) and one indirect jump lands on its body:
+//     every lane of a warp takes the same branch, so there is no divergence,
+//     only the jump itself per (j, i) pair;
 //   * a warp owns 1 KiB of every shard per step (lane l holds 16-byte vectors
 //     l and l+32), transposes each input's eight words into bit-planes (three
-//     delta-swap stages), keeps 4 x 8 accumulator planes in registers per
-//     pass over the inputs, and transposes them back.
+//     delta-swap stages), forms the XORs of all subsets of its low and high
+//     four planes (so each row of a body is one three-input XOR), keeps
+//     4 x 8 accumulator planes in registers per pass over the inputs, and
+//     transposes them back.
 //
 // Register arrays cannot be indexed by a run-time input number, and inlining
-// one 256-way switch per (output, input) pair makes the code, and ptxas's time
-// (quadratic in the copies), explode.  So a warp's inputs are staged raw in
+// the 256 bodies once per (output, input) pair makes the code, and ptxas's
+// time (quadratic in the copies), explode.  So a warp's inputs are staged raw in
 // a ring of 1 KiB slots in shared memory with cp.async: each lane owns its
 // own 16-byte slots (no synchronisation, no bank conflicts), the input loop
-// stays rolled, and the kernel holds exactly four switch copies (one per
-// accumulated output).  The next chunk's inputs are copied into the slots as
+// stays rolled, and the kernel holds exactly four copies of the bodies (one
+// per accumulated output).  The next chunk's inputs are copied into the slots as
 // this chunk consumes them, so loads overlap the arithmetic.
 //
 // Any decode matrix (Reconstruct, ReconstructData, ReconstructSome, DecodeIdx)
@@ -35,9 +36,8 @@
 #pragma once
 
 #include <cstdint>
-#include <type_traits>
-#include <utility>
 
+#include "gf8_rt_dispatch.inc"
 #include "kernels.h"
 
 namespace rsgpu {
@@ -46,67 +46,41 @@ namespace gf8rt {
 constexpr int kChunk = 1024;  // bytes of every shard per warp step
 constexpr int kPass = 4;      // outputs accumulated in registers per pass over the inputs
 
-// GF(2^8) product, polynomial 0x11D (galois.go's field), at compile time.
-constexpr uint32_t cmul(uint32_t a, uint32_t b) {
-    uint32_t r = 0;
-    for (int i = 0; i < 8; i++) {
-        if (b & 1u) r ^= a;
-        b >>= 1;
-        a = (a << 1) ^ ((a & 0x80u) ? 0x11Du : 0u);
-    }
-    return r & 0xFFu;
-}
-
-// Bit (8b + a) set when plane a of x feeds plane b of c*x.
-constexpr uint64_t bitmat(uint32_t c) {
-    uint64_t m = 0;
-    for (int a = 0; a < 8; a++) {
-        const uint32_t col = cmul(c, 1u << a);
-        for (int b = 0; b < 8; b++)
-            if ((col >> b) & 1u) m |= 1ull << (8 * b + a);
-    }
-    return m;
-}
-
-// y ^= C * x on bit-planes.  Each row is one XOR chain that the compiler
-// fuses into three-input LOP3s.
-template <int C>
-__device__ __forceinline__ void mul_acc(uint32_t (&y)[8], const uint32_t (&x)[8]) {
-    constexpr uint64_t M = bitmat((uint32_t)C);
+// The XORs of every non-empty subset of x's planes 0-3 (t[m-1] = lo[m]) and
+// of planes 4-7 (t[14+m] = hi[m]), m = 1..15: 22 XORs per input, shared by
+// all the outputs it feeds.
+__device__ __forceinline__ void subset_xors(const uint32_t (&x)[8], uint32_t (&t)[30]) {
 #pragma unroll
-    for (int b = 0; b < 8; b++) {
-        uint32_t t = y[b];
+    for (int h = 0; h < 2; h++) {
+        uint32_t *T = t + 15 * h;  // T[m-1]
+        const uint32_t *w = x + 4 * h;
+        T[0] = w[0];
+        T[1] = w[1];
+        T[2] = w[0] ^ w[1];
+        T[3] = w[2];
+        T[4] = w[2] ^ w[0];
+        T[5] = w[2] ^ w[1];
+        T[6] = w[2] ^ T[2];
+        T[7] = w[3];
 #pragma unroll
-        for (int a = 0; a < 8; a++)
-            if ((M >> (8 * b + a)) & 1ull) t ^= x[a];
-        y[b] = t;
+        for (int m = 1; m < 8; m++) T[7 + m] = w[3] ^ T[m - 1];
     }
 }
 
-#define RSGPU_RT_CASE(n)  \
-    case n:               \
-        mul_acc<n>(y, x); \
-        break;
-#define RSGPU_RT_CASE16(h)                                                          \
-    RSGPU_RT_CASE(h * 16 + 0) RSGPU_RT_CASE(h * 16 + 1) RSGPU_RT_CASE(h * 16 + 2)   \
-    RSGPU_RT_CASE(h * 16 + 3) RSGPU_RT_CASE(h * 16 + 4) RSGPU_RT_CASE(h * 16 + 5)   \
-    RSGPU_RT_CASE(h * 16 + 6) RSGPU_RT_CASE(h * 16 + 7) RSGPU_RT_CASE(h * 16 + 8)   \
-    RSGPU_RT_CASE(h * 16 + 9) RSGPU_RT_CASE(h * 16 + 10) RSGPU_RT_CASE(h * 16 + 11) \
-    RSGPU_RT_CASE(h * 16 + 12) RSGPU_RT_CASE(h * 16 + 13) RSGPU_RT_CASE(h * 16 + 14) \
-    RSGPU_RT_CASE(h * 16 + 15)
-
-// y ^= c * x for a warp-uniform run-time coefficient c (c = 0: nothing).
-__device__ __forceinline__ void mul_acc_rt(uint32_t c, uint32_t (&y)[8], const uint32_t (&x)[8]) {
-    switch (c & 0xFFu) {
-        case 0:
-            break;
-        RSGPU_RT_CASE(1) RSGPU_RT_CASE(2) RSGPU_RT_CASE(3) RSGPU_RT_CASE(4) RSGPU_RT_CASE(5)
-        RSGPU_RT_CASE(6) RSGPU_RT_CASE(7) RSGPU_RT_CASE(8) RSGPU_RT_CASE(9) RSGPU_RT_CASE(10)
-        RSGPU_RT_CASE(11) RSGPU_RT_CASE(12) RSGPU_RT_CASE(13) RSGPU_RT_CASE(14) RSGPU_RT_CASE(15)
-        RSGPU_RT_CASE16(1) RSGPU_RT_CASE16(2) RSGPU_RT_CASE16(3) RSGPU_RT_CASE16(4) RSGPU_RT_CASE16(5)
-        RSGPU_RT_CASE16(6) RSGPU_RT_CASE16(7) RSGPU_RT_CASE16(8) RSGPU_RT_CASE16(9) RSGPU_RT_CASE16(10)
-        RSGPU_RT_CASE16(11) RSGPU_RT_CASE16(12) RSGPU_RT_CASE16(13) RSGPU_RT_CASE16(14) RSGPU_RT_CASE16(15)
-    }
+// y ^= c * x on bit-planes for a warp-uniform run-time coefficient c
+// (0..255), given x's subset XORs t.  One indirect jump (PTX brx.idx over a
+// list of 256 labels) lands on the body for c: row b of c*x XORs the planes
+// of a fixed mask, i.e. lo[mask & 15] ^ hi[mask >> 4], so a body is at most
+// eight three-input XORs (none for c = 0).  The bodies are generated at build
+// time (gen_rt_dispatch.py); a C++ switch over the same cases compiles to a
+// binary compare tree of about nine levels instead of one jump.
+__device__ __forceinline__ void mul_acc_rt(uint32_t c, uint32_t (&y)[8], const uint32_t (&t)[30]) {
+    asm(RSGPU_RT_DISPATCH_ASM
+        : "+r"(y[0]), "+r"(y[1]), "+r"(y[2]), "+r"(y[3]), "+r"(y[4]), "+r"(y[5]), "+r"(y[6]), "+r"(y[7])
+        : "r"(t[0]), "r"(t[1]), "r"(t[2]), "r"(t[3]), "r"(t[4]), "r"(t[5]), "r"(t[6]), "r"(t[7]), "r"(t[8]),
+          "r"(t[9]), "r"(t[10]), "r"(t[11]), "r"(t[12]), "r"(t[13]), "r"(t[14]), "r"(t[15]), "r"(t[16]),
+          "r"(t[17]), "r"(t[18]), "r"(t[19]), "r"(t[20]), "r"(t[21]), "r"(t[22]), "r"(t[23]), "r"(t[24]),
+          "r"(t[25]), "r"(t[26]), "r"(t[27]), "r"(t[28]), "r"(t[29]), "r"(c & 0xFFu));
 }
 
 // Exchanges bits (m << s) of x with bits m of y (one delta swap).
@@ -127,24 +101,12 @@ __device__ __forceinline__ void t8(uint32_t (&w)[8]) {
     dswap(w[4], w[5], 0x55555555u, 1); dswap(w[6], w[7], 0x55555555u, 1);
 }
 
-// Calls f(std::integral_constant<int, 0..N-1>) in order.  The loop bodies
-// below hold whole 256-way switches, far beyond what the compiler's loop
-// unroller accepts; unrolling them here keeps every register array indexed
-// by constants (a loop left rolled would move the arrays to local memory).
-template <typename F, int... Is>
-__device__ __forceinline__ void sfor_impl(F &&f, std::integer_sequence<int, Is...>) {
-    (f(std::integral_constant<int, Is>{}), ...);
-}
-template <int N, typename F>
-__device__ __forceinline__ void sfor(F &&f) {
-    sfor_impl(f, std::make_integer_sequence<int, N>{});
-}
-
 __device__ __forceinline__ void cp_async16(uint32_t smem_addr, const void *gptr) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr), "l"(gptr) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
+// A lane's 32 bytes of one ring slot: 16-byte pieces at sa and sa + 512.
 __device__ __forceinline__ void lds2(uint32_t sa, uint32_t (&x)[8]) {
     asm volatile("ld.shared.v4.u32 {%0,%1,%2,%3}, [%4];" : "=r"(x[0]), "=r"(x[1]), "=r"(x[2]), "=r"(x[3]) : "r"(sa));
     asm volatile("ld.shared.v4.u32 {%0,%1,%2,%3}, [%4];"
@@ -180,6 +142,34 @@ __device__ __forceinline__ void finish_output(uint32_t (&y)[8], uint4 *dst, long
     }
 }
 
+// One pass over the inputs for outputs j0..j0+3 (all four exist when kFull;
+// otherwise outputs from n_out on are skipped).  See bitslice_step.
+template <bool kFull, typename CoefFn, typename NextFn>
+__device__ __forceinline__ void bitslice_pass(uint32_t (&y)[kPass][8], uint32_t ring_s, int base, int ring, int lane,
+                                              int n_in, int n_out, int j0, bool first, bool last, int ahead,
+                                              CoefFn coef, NextFn issue_next) {
+    int slot = base;
+    for (int i = 0; i < n_in; i++) {
+        const uint32_t sa = ring_s + (uint32_t)(slot * kChunk + lane * 16);
+        uint32_t x[8];
+        lds2(sa, x);
+        if (first) {
+            t8(x);
+            if (!last) sts2(sa, x);
+        }
+        uint32_t t[30];
+        subset_xors(x, t);
+        mul_acc_rt(coef(j0, i), y[0], t);
+        if (kFull || j0 + 1 < n_out) mul_acc_rt(coef(j0 + 1, i), y[1], t);
+        if (kFull || j0 + 2 < n_out) mul_acc_rt(coef(j0 + 2, i), y[2], t);
+        if (kFull || j0 + 3 < n_out) mul_acc_rt(coef(j0 + 3, i), y[3], t);
+        // x has been consumed (the products depend on it), so the slot may
+        // be overwritten by the next chunk's copy.
+        if (last && i + ahead < n_in) issue_next(i + ahead, sa);
+        slot = slot + 1 == ring ? 0 : slot + 1;
+    }
+}
+
 // One warp's step over chunk c (1 KiB of every shard) whose raw input vectors
 // have landed in the warp's ring (slot of input i: (base + i) mod ring).
 // Outputs are produced kPass at a time; with more than one pass the first
@@ -195,27 +185,18 @@ __device__ __forceinline__ void bitslice_step(uint32_t ring_s, int base, int rin
         const bool last = pass + 1 == npass;
         const int j0 = pass * kPass;
         uint32_t y[kPass][8];
-        sfor<kPass>([&](auto J) { sfor<8>([&](auto B) { y[J][B] = 0; }); });
-        int slot = base;
-        for (int i = 0; i < n_in; i++) {
-            const uint32_t sa = ring_s + (uint32_t)(slot * kChunk + lane * 16);
-            uint32_t x[8];
-            lds2(sa, x);
-            if (pass == 0) {
-                t8(x);
-                if (!last) sts2(sa, x);
-            }
-            sfor<kPass>([&](auto J) {
-                if (j0 + J < n_out) mul_acc_rt(coef(j0 + J, i), y[J], x);
-            });
-            // x has been consumed (the products depend on it), so the slot
-            // may be overwritten by the next chunk's copy.
-            if (last && i + ahead < n_in) issue_next(i + ahead, sa);
-            slot = slot + 1 == ring ? 0 : slot + 1;
-        }
-        sfor<kPass>([&](auto J) {
-            if (j0 + J < n_out) finish_output(y[J], out(j0 + J), v0, mode, diff);
-        });
+#pragma unroll
+        for (int j = 0; j < kPass; j++)
+#pragma unroll
+            for (int b = 0; b < 8; b++) y[j][b] = 0;
+        if (j0 + kPass <= n_out)
+            bitslice_pass<true>(y, ring_s, base, ring, lane, n_in, n_out, j0, pass == 0, last, ahead, coef, issue_next);
+        else
+            bitslice_pass<false>(y, ring_s, base, ring, lane, n_in, n_out, j0, pass == 0, last, ahead, coef, issue_next);
+        finish_output(y[0], out(j0), v0, mode, diff);
+        if (j0 + 1 < n_out) finish_output(y[1], out(j0 + 1), v0, mode, diff);
+        if (j0 + 2 < n_out) finish_output(y[2], out(j0 + 2), v0, mode, diff);
+        if (j0 + 3 < n_out) finish_output(y[3], out(j0 + 3), v0, mode, diff);
     }
 }
 
@@ -233,7 +214,7 @@ __global__ void __launch_bounds__(512, 1) gf8_bitslice_kernel(const __grid_const
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
     long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     auto issue = [&](long long chunk, int i, uint32_t sa) {
-        const uint4 *p = reinterpret_cast<const uint4 *>(a.in[i]) + chunk * 64 + lane;
+        const uint4 *p = reinterpret_cast<const uint4 *>(a.in[i]) + chunk * (kChunk / 16) + lane;
         cp_async16(sa, p);
         cp_async16(sa + 512, p + 32);
     };
@@ -255,7 +236,7 @@ __global__ void __launch_bounds__(512, 1) gf8_bitslice_kernel(const __grid_const
             }
         }
         bitslice_step(
-            ring_s, base, ring, lane, n_in, n_out, ahead, mode, c * 64 + lane,
+            ring_s, base, ring, lane, n_in, n_out, ahead, mode, c * (kChunk / 16) + lane,
             [&](int j, int i) -> uint32_t { return a.coef[j][i]; },
             [&](int j) { return reinterpret_cast<uint4 *>(a.out[j]); },
             [&](int i, uint32_t sa) {

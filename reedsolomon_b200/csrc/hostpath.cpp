@@ -117,9 +117,14 @@ extern "C" int rsgpu_encode_host(rsgpu_encoder *enc, uint8_t *const *host, size_
     });
 }
 
-extern "C" int rsgpu_reconstruct_host(rsgpu_encoder *enc, uint8_t **host, const uint8_t *present,
-                                      size_t size, int data_only, uint8_t *written) {
-    RS_TRACE("rsgpu_reconstruct_host");
+namespace {
+
+// Host-buffer Reconstruct / ReconstructData / ReconstructSome: the inputs
+// (the first k present shards, classic; every present shard, Leopard) go
+// H2D, the rebuilt shards D2H, per column chunk.  Host outputs must be
+// preallocated.
+int reconstruct_host_common(rsgpu_encoder *enc, uint8_t **host, const uint8_t *present, size_t size, int data_only,
+                            const uint8_t *required, int n_required, uint8_t *written) {
     if (!enc) return RS_ERR_INVALID_INPUT;
     if (!enc->ctx) return RS_ERR_NO_DEVICE;
     if (!host || !present) return RS_ERR_TOO_FEW_SHARDS;
@@ -129,6 +134,9 @@ extern "C" int rsgpu_reconstruct_host(rsgpu_encoder *enc, uint8_t **host, const 
     std::lock_guard<std::recursive_mutex> lk(ctx->mu);
     if (enc->codec != RS_CODEC_CLASSIC) {
         if (size % 64) return RS_ERR_INVALID_SHARD_SIZE;
+        // leopard.go:378-391: ReconstructSome recovers parity only when
+        // required covers every shard; it is otherwise data-only.
+        if (required) data_only = n_required != enc->total;
         std::vector<int> ins, outs;
         int np = 0, dp = 0;
         for (int i = 0; i < enc->total; i++) {
@@ -157,7 +165,7 @@ extern "C" int rsgpu_reconstruct_host(rsgpu_encoder *enc, uint8_t **host, const 
     }
     std::vector<uint8_t> dec_rows;
     std::vector<int> out_idx, in_idx;
-    int rc = classic_decode_plan(enc, present, data_only, nullptr, 0, dec_rows, out_idx, in_idx);
+    int rc = classic_decode_plan(enc, present, data_only, required, n_required, dec_rows, out_idx, in_idx);
     if (rc || out_idx.empty()) return rc;
     for (int i : in_idx)
         if (!host[i]) return RS_ERR_SHARD_SIZE;
@@ -184,4 +192,225 @@ extern "C" int rsgpu_reconstruct_host(rsgpu_encoder *enc, uint8_t **host, const 
     if (rc == RS_OK && written)
         for (int o : out_idx) written[o] = 1;
     return rc;
+}
+
+}  // namespace
+
+extern "C" int rsgpu_reconstruct_host(rsgpu_encoder *enc, uint8_t **host, const uint8_t *present,
+                                      size_t size, int data_only, uint8_t *written) {
+    RS_TRACE("rsgpu_reconstruct_host");
+    return reconstruct_host_common(enc, host, present, size, data_only, nullptr, 0, written);
+}
+
+extern "C" int rsgpu_reconstruct_some_host(rsgpu_encoder *enc, uint8_t **host, const uint8_t *present,
+                                           const uint8_t *required, int n_required, size_t size,
+                                           uint8_t *written) {
+    RS_TRACE("rsgpu_reconstruct_some_host");
+    if (!enc) return RS_ERR_INVALID_INPUT;
+    // reedsolomon.go:1655-1660
+    if (!required || (n_required != enc->k && n_required != enc->total)) return RS_ERR_INVALID_INPUT;
+    return reconstruct_host_common(enc, host, present, size, n_required == enc->k, required, n_required,
+                                   written);
+}
+
+extern "C" int rsgpu_verify_host(rsgpu_encoder *enc, uint8_t *const *host, size_t size, int *ok) {
+    RS_TRACE("rsgpu_verify_host");
+    if (!enc || !ok) return RS_ERR_INVALID_INPUT;
+    if (!enc->ctx) return RS_ERR_NO_DEVICE;
+    *ok = 0;
+    if (!host) return RS_ERR_TOO_FEW_SHARDS;
+    for (int i = 0; i < enc->total; i++)
+        if (!host[i]) return RS_ERR_SHARD_SIZE;
+    if (size == 0) return RS_ERR_SHARD_NO_DATA;
+    if (enc->p == 0) {
+        *ok = 1;
+        return RS_OK;
+    }
+    rsgpu_ctx *ctx = enc->ctx;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    const int k = enc->k, p = enc->p, total = enc->total;
+    // every shard goes H2D; nothing comes back but the mismatch flag
+    std::vector<uint8_t *> rows(host, host + total);
+    std::vector<int> ins, outs;
+    for (int i = 0; i < total; i++) ins.push_back(i);
+    RS_CUDA(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
+    int rc;
+    if (enc->codec != RS_CODEC_CLASSIC) {
+        if (size % 64) return RS_ERR_INVALID_SHARD_SIZE;
+        // Leopard (leopard.go:393-419): re-encode into p staging rows past the
+        // shards (never copied), then compare them with the received parity.
+        for (int i = 0; i < p; i++) rows.push_back(nullptr);
+        rc = run_pipeline(ctx, rows, ins, outs, size, 64, [&](std::vector<uint8_t *> &dev, size_t len) {
+            std::vector<uint8_t *> tmp(dev.begin(), dev.begin() + total);
+            for (int i = 0; i < p; i++) tmp[k + i] = dev[total + i];
+            int r = leo_encode_enqueue(enc, tmp.data(), len);
+            if (r) return r;
+            const uint8_t one = 1;
+            for (int i = 0; i < p; i++) {
+                const uint8_t *src = dev[total + i];
+                RS_CUDA(launch_gf8_matmul(ctx->stream, ctx->info, &one, 1, 1, &src, &dev[k + i], len, kModeVerify,
+                                          ctx->d_flag));
+            }
+            return RS_OK;
+        });
+    } else {
+        // reedsolomon.go:857-871 with checkSomeShards fused: parity compared in place
+        rc = run_pipeline(ctx, rows, ins, outs, size, 16, [&](std::vector<uint8_t *> &dev, size_t len) {
+            RS_CUDA(launch_gf8_matmul(ctx->stream, ctx->info, enc->parity_rows.data(), k, p,
+                                      (const uint8_t *const *)dev.data(), dev.data() + k, len, kModeVerify,
+                                      ctx->d_flag));
+            return RS_OK;
+        });
+    }
+    if (rc) return rc;
+    RS_CUDA(cudaMemcpyAsync(ctx->h_flag, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    RS_CUDA(cudaStreamSynchronize(ctx->stream));
+    *ok = (*ctx->h_flag == 0);
+    return RS_OK;
+}
+
+extern "C" int rsgpu_encode_idx_host(rsgpu_encoder *enc, const uint8_t *host_data, int idx, uint8_t *const *host_parity,
+                                     size_t size) {
+    RS_TRACE("rsgpu_encode_idx_host");
+    if (!enc) return RS_ERR_INVALID_INPUT;
+    if (!enc->ctx) return RS_ERR_NO_DEVICE;
+    if (enc->codec != RS_CODEC_CLASSIC) return RS_ERR_NOT_SUPPORTED;  // leopard.go:272
+    if (enc->p == 0) return RS_OK;
+    if (idx < 0 || idx >= enc->k) return RS_ERR_INV_SHARD_NUM;
+    if (!host_parity) return RS_ERR_TOO_FEW_SHARDS;
+    for (int o = 0; o < enc->p; o++)
+        if (!host_parity[o]) return RS_ERR_SHARD_SIZE;
+    if (!host_data) return RS_ERR_SHARD_SIZE;
+    if (size == 0) return RS_ERR_SHARD_NO_DATA;
+    rsgpu_ctx *ctx = enc->ctx;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    const int p = enc->p;
+    // parity[o] ^= M[k+o][idx] * data (reedsolomon.go:708-757): the data and
+    // the parity go H2D, the parity comes back
+    std::vector<uint8_t> col(p);
+    for (int o = 0; o < p; o++) col[o] = enc->parity_rows[(size_t)o * enc->k + idx];
+    std::vector<uint8_t *> rows{const_cast<uint8_t *>(host_data)};
+    std::vector<int> ins{0}, outs;
+    for (int o = 0; o < p; o++) {
+        rows.push_back(host_parity[o]);
+        ins.push_back(1 + o);
+        outs.push_back(1 + o);
+    }
+    return run_pipeline(ctx, rows, ins, outs, size, 16, [&](std::vector<uint8_t *> &dev, size_t len) {
+        RS_CUDA(launch_gf8_matmul(ctx->stream, ctx->info, col.data(), 1, p, (const uint8_t *const *)dev.data(),
+                                  dev.data() + 1, len, kModeXor, ctx->d_flag));
+        return RS_OK;
+    });
+}
+
+extern "C" int rsgpu_update_host(rsgpu_encoder *enc, uint8_t *const *host, const uint8_t *const *host_new,
+                                 size_t size) {
+    RS_TRACE("rsgpu_update_host");
+    if (!enc) return RS_ERR_INVALID_INPUT;
+    if (!enc->ctx) return RS_ERR_NO_DEVICE;
+    if (enc->codec != RS_CODEC_CLASSIC) return RS_ERR_NOT_SUPPORTED;  // leopard.go:316, leopard8.go:289
+    if (!host || !host_new) return RS_ERR_TOO_FEW_SHARDS;
+    if (size == 0) return RS_ERR_SHARD_NO_DATA;
+    const int k = enc->k, p = enc->p;
+    std::vector<int> cols;
+    for (int c = 0; c < k; c++)
+        if (host_new[c]) {
+            if (!host[c]) return RS_ERR_INVALID_INPUT;
+            cols.push_back(c);
+        }
+    if (cols.empty()) return RS_ERR_SHARD_NO_DATA;  // checkShards(newDatashards, true)
+    for (int o = 0; o < p; o++)
+        if (!host[k + o]) return RS_ERR_INVALID_INPUT;
+    if (p == 0) return RS_OK;
+    rsgpu_ctx *ctx = enc->ctx;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    // reedsolomon.go:762-853: rows [0,n) the changed shards (left holding the
+    // delta, like the reference), [n,2n) their new data, [2n,2n+p) parity
+    const int n = (int)cols.size();
+    std::vector<uint8_t> prow((size_t)p * n);
+    std::vector<uint8_t *> rows;
+    std::vector<int> ins, outs;
+    for (int j = 0; j < n; j++) {
+        rows.push_back(host[cols[j]]);
+        ins.push_back(j);
+        outs.push_back(j);
+        for (int o = 0; o < p; o++) prow[(size_t)o * n + j] = enc->parity_rows[(size_t)o * k + cols[j]];
+    }
+    for (int j = 0; j < n; j++) {
+        rows.push_back(const_cast<uint8_t *>(host_new[cols[j]]));
+        ins.push_back(n + j);
+    }
+    for (int o = 0; o < p; o++) {
+        rows.push_back(host[k + o]);
+        ins.push_back(2 * n + o);
+        outs.push_back(2 * n + o);
+    }
+    return run_pipeline(ctx, rows, ins, outs, size, 16, [&](std::vector<uint8_t *> &dev, size_t len) {
+        for (int j = 0; j < n; j++) RS_CUDA(launch_xor(ctx->stream, ctx->info, dev[n + j], dev[j], len));
+        RS_CUDA(launch_gf8_matmul(ctx->stream, ctx->info, prow.data(), n, p, (const uint8_t *const *)dev.data(),
+                                  dev.data() + 2 * n, len, kModeXor, ctx->d_flag));
+        return RS_OK;
+    });
+}
+
+extern "C" int rsgpu_decode_idx_host(rsgpu_encoder *enc, uint8_t *const *host_dst, const uint8_t *expect,
+                                     const uint8_t *const *host_input, size_t size) {
+    RS_TRACE("rsgpu_decode_idx_host");
+    if (!enc) return RS_ERR_INVALID_INPUT;
+    if (!enc->ctx) return RS_ERR_NO_DEVICE;
+    if (enc->codec != RS_CODEC_CLASSIC) return RS_ERR_NOT_SUPPORTED;  // leopard.go:94, leopard8.go:90
+    if (!host_dst || !host_input) return RS_ERR_INVALID_INPUT;
+    rsgpu_ctx *ctx = enc->ctx;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    const int total = enc->total;
+    std::vector<uint8_t *> rows;
+    std::vector<int> ins, outs;
+    if (!expect) {  // merging mode: dst[i] ^= input[i]
+        for (int i = 0; i < total; i++)
+            if (host_input[i] && !host_dst[i]) return RS_ERR_INVALID_INPUT;
+        if (size == 0) return RS_OK;
+        std::vector<int> pairs;
+        for (int i = 0; i < total; i++)
+            if (host_input[i]) pairs.push_back(i);
+        if (pairs.empty()) return RS_OK;
+        const int n = (int)pairs.size();
+        for (int j = 0; j < n; j++) {
+            rows.push_back(const_cast<uint8_t *>(host_input[pairs[j]]));
+            ins.push_back(j);
+        }
+        for (int j = 0; j < n; j++) {
+            rows.push_back(host_dst[pairs[j]]);
+            ins.push_back(n + j);
+            outs.push_back(n + j);
+        }
+        return run_pipeline(ctx, rows, ins, outs, size, 16, [&](std::vector<uint8_t *> &dev, size_t len) {
+            for (int j = 0; j < n; j++) RS_CUDA(launch_xor(ctx->stream, ctx->info, dev[j], dev[n + j], len));
+            return RS_OK;
+        });
+    }
+    std::vector<uint8_t> has_in(total), has_dst(total);
+    for (int i = 0; i < total; i++) {
+        has_in[i] = host_input[i] != nullptr;
+        has_dst[i] = host_dst[i] != nullptr;
+    }
+    std::vector<uint8_t> dec_rows;
+    std::vector<int> in_sh, out_sh;
+    int rc = decode_idx_plan(enc, expect, has_in.data(), has_dst.data(), dec_rows, in_sh, out_sh);
+    if (rc || in_sh.empty() || out_sh.empty() || size == 0) return rc;
+    const int n_in = (int)in_sh.size(), n_out = (int)out_sh.size();
+    for (int j = 0; j < n_in; j++) {
+        rows.push_back(const_cast<uint8_t *>(host_input[in_sh[j]]));
+        ins.push_back(j);
+    }
+    for (int o = 0; o < n_out; o++) {  // accumulated: read, updated, written back
+        rows.push_back(host_dst[out_sh[o]]);
+        ins.push_back(n_in + o);
+        outs.push_back(n_in + o);
+    }
+    return run_pipeline(ctx, rows, ins, outs, size, 16, [&](std::vector<uint8_t *> &dev, size_t len) {
+        RS_CUDA(launch_gf8_matmul(ctx->stream, ctx->info, dec_rows.data(), n_in, n_out,
+                                  (const uint8_t *const *)dev.data(), dev.data() + n_in, len, kModeXor,
+                                  ctx->d_flag));
+        return RS_OK;
+    });
 }

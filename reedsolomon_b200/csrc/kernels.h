@@ -77,6 +77,18 @@ cudaError_t launch_gf8_matmul(cudaStream_t st, const DeviceInfo &dev, const uint
 cudaError_t launch_bitslice(cudaStream_t st, const DeviceInfo &dev, const GfMatArgs &a, int mode,
                             long long *bytes_done);
 
+// launch_gf8_matmul restricted to a fixed set of table kernels (one per
+// output-group count and mode, plus the byte kernel for tails), chosen
+// without the tuner and without occupancy queries.  After
+// preload_static_kernels() has run on a device, launches of this set load no
+// code there (with lazy module loading a kernel's first launch loads its
+// module, which allocates device memory).
+cudaError_t launch_gf8_matmul_static(cudaStream_t st, const DeviceInfo &dev, const uint8_t *rows, int n_in,
+                                     int n_out, const uint8_t *const *in, uint8_t *const *out, size_t nbytes,
+                                     int mode, int *d_flag);
+// Loads every kernel launch_gf8_matmul_static can launch on the current device.
+cudaError_t preload_static_kernels();
+
 // Fill an 8-byte aligned buffer with uniform pseudo-random bytes (tuning inputs).
 cudaError_t launch_fill_random(cudaStream_t st, const DeviceInfo &dev, uint8_t *p, size_t nbytes,
                                uint64_t seed);

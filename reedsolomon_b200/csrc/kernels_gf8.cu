@@ -382,6 +382,71 @@ cudaError_t launch_gf8_matmul(cudaStream_t st, const DeviceInfo &dev, const uint
     return cudaSuccess;
 }
 
+// The fixed kernel set of launch_gf8_matmul_static: the PRMT-addressed
+// table kernel (input loop not unrolled, so one kernel serves every input
+// count) and the byte kernel, per output-group count and mode.
+namespace {
+constexpr int kStaticBlocksPerSm = 4;  // grid cap; the kernels loop over what is left
+
+void static_kernels(int G, int mode, VecKernel *vk, ByteKernel *bk) {
+    *vk = vec_kernel(G, mode, kVariantPrmt);
+    *bk = byte_kernel(G, mode);
+}
+}  // namespace
+
+cudaError_t preload_static_kernels() {
+    for (int G = 1; G <= 4; G++)
+        for (int mode = kModeWrite; mode <= kModeVerify; mode++) {
+            VecKernel vk;
+            ByteKernel bk;
+            static_kernels(G, mode, &vk, &bk);
+            cudaFuncAttributes fa;
+            cudaError_t e = cudaFuncGetAttributes(&fa, (const void *)vk);
+            if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, (const void *)bk);
+            if (e != cudaSuccess) return e;
+        }
+    return cudaSuccess;
+}
+
+cudaError_t launch_gf8_matmul_static(cudaStream_t st, const DeviceInfo &dev, const uint8_t *rows, int n_in,
+                                     int n_out, const uint8_t *const *in, uint8_t *const *out, size_t nbytes,
+                                     int mode, int *d_flag) {
+    if (n_in <= 0 || n_out <= 0 || nbytes == 0) return cudaSuccess;
+    for (int o0 = 0; o0 < n_out; o0 += kMaxOut) {
+        const int no = std::min(kMaxOut, n_out - o0);
+        for (int i0 = 0; i0 < n_in; i0 += kMaxIn) {
+            const int ni = std::min(kMaxIn, n_in - i0);
+            GfMatArgs a;
+            fill_args(a, rows + (size_t)o0 * n_in + i0, n_in, ni, no, in + i0, out + o0, nbytes, d_flag);
+            const int m = (mode == kModeWrite && i0 > 0) ? kModeXor : mode;
+            const int G = (no + 3) / 4;
+            const size_t smem = (size_t)ni * kInStride + kTableAlign;
+            VecKernel vk;
+            ByteKernel bk;
+            static_kernels(G, m, &vk, &bk);
+            bool vec_ok = true;
+            for (int i = 0; i < ni; i++) vec_ok &= aligned16(a.in[i]);
+            for (int o = 0; o < no; o++) vec_ok &= aligned16(a.out[o]);
+            long long done = 0;
+            const long long cap = (long long)dev.sm_count * kStaticBlocksPerSm;
+            if (vec_ok && (a.nbytes >> 4) > 0) {
+                const long long nvec = a.nbytes >> 4;
+                const int grid = (int)std::max(1LL, std::min((nvec + kThreads - 1) / kThreads, cap));
+                vk<<<grid, kThreads, smem, st>>>(a);
+                done = nvec << 4;
+            }
+            if (done < a.nbytes) {
+                const long long rem = a.nbytes - done;
+                const int grid = (int)std::max(1LL, std::min((rem + kThreads - 1) / kThreads, cap));
+                bk<<<grid, kThreads, smem, st>>>(a, done);
+            }
+            cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) return e;
+        }
+    }
+    return cudaSuccess;
+}
+
 cudaError_t launch_fill_random(cudaStream_t st, const DeviceInfo &dev, uint8_t *p, size_t nbytes,
                                uint64_t seed) {
     const long long nwords = (long long)(nbytes / 8);

@@ -3,9 +3,10 @@
 //
 // Shape: one CTA per SM (grid = SM count, or fewer for small shards), up to
 // 16 warps per CTA; every warp keeps a ring of n_in + ahead 1 KiB slots in
-// dynamic shared memory, so wide input counts get fewer warps (32 inputs:
-// 35 KiB per warp, 6 warps in 227 KiB).  Algorithmic bytes per launch:
-// (n_in + n_out) * nbytes (+ n_out * nbytes read in xor / verify modes).
+// dynamic shared memory, so wide input counts get fewer warps (RS(10,4):
+// 13 KiB per warp, 16 warps; 32 inputs: 35 KiB, 6 warps).  Algorithmic bytes per
+// launch: (n_in + n_out) * nbytes (+ n_out * nbytes read in xor / verify
+// modes).
 #include <algorithm>
 #include <mutex>
 
@@ -14,7 +15,7 @@
 namespace rsgpu {
 namespace {
 
-constexpr int kMaxWarps = 16;
+constexpr int kMaxWarps = 16;  // the kernel is compiled for at most 512 threads per CTA
 constexpr int kAhead = 3;  // next-chunk inputs issued before the last pass starts
 constexpr int kMaxDevices = 64;
 

@@ -9,10 +9,19 @@
 // a flag and grows a scratch buffer); this entry point needs neither.
 //
 // Its only scratch memory is g_noalloc_scratch below, a file-scope device
-// array of kNoAllocScratchBytes (8 MiB).  Every GPU that loads librsgpu.so
-// holds that array until the process exits.  It holds the mismatch flag and,
+// array of kNoAllocScratchBytes (8 MiB).  It holds the mismatch flag and,
 // when there are more inputs than one kernel launch takes (32), the partial
 // parity rows; calls whose partial rows would not fit are rejected.
+//
+// Device memory is also taken when code is loaded: with lazy module loading
+// (the CUDA default) a module is loaded, and its memory allocated, when one
+// of its symbols is first used.  So the first call on a device does all of
+// that up front: it looks up the array's device address (which loads this
+// file's module, array included) and loads every kernel this entry point can
+// launch (a fixed set of table kernels, the same for every geometry).  From
+// then on, calls on that device allocate nothing.  Callers should make one
+// call at start-up, before any stream capture; every GPU that has run it
+// holds the array and the loaded code until the process exits.
 #include <cstring>
 #include <mutex>
 
@@ -24,9 +33,6 @@ namespace {
 constexpr size_t kNoAllocScratchBytes = 8u << 20;  // per device
 constexpr size_t kFlagBytes = 256;                 // mismatch flag, padded to keep rows aligned
 constexpr int kMaxDevices = 64;
-// Only the table kernels: the run-time compiled XOR-network kernels load a
-// module on first use, which allocates device memory.
-constexpr bool kTableKernelsOnly = false;
 
 __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocScratchBytes];
 
@@ -36,8 +42,8 @@ DeviceInfo g_info[kMaxDevices];
 bool g_ready[kMaxDevices];
 
 // Once per device, with that device current: the device address of the
-// array (in host code the symbol itself is only a host-side stand-in) and the
-// SM count used to size grids.
+// array (in host code the symbol itself is only a host-side stand-in), the
+// SM count used to size grids, and every kernel the calls launch loaded.
 int device_scratch(uint8_t **scratch, DeviceInfo *info) {
     int dev = 0;
     RS_CUDA(cudaGetDevice(&dev));
@@ -48,6 +54,7 @@ int device_scratch(uint8_t **scratch, DeviceInfo *info) {
         RS_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
         int sms = 0;
         RS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        RS_CUDA(preload_static_kernels());
         g_scratch_addr[dev] = (uint8_t *)p;
         g_info[dev].device = dev;
         g_info[dev].sm_count = sms;
@@ -88,8 +95,8 @@ extern "C" int rsgpu_check_some_shards_noalloc(const uint8_t *rows, int n_in, in
     // The array keeps the previous call's contents: the flag must start at 0.
     RS_CUDA(cudaMemsetAsync(d_flag, 0, sizeof(int), st));
     if (n_in <= kMaxIn) {
-        RS_CUDA(launch_gf8_matmul(st, info, rows, n_in, n_out, in, const_cast<uint8_t *const *>(to_check),
-                                  nbytes, kModeVerify, d_flag, kTableKernelsOnly));
+        RS_CUDA(launch_gf8_matmul_static(st, info, rows, n_in, n_out, in,
+                                         const_cast<uint8_t *const *>(to_check), nbytes, kModeVerify, d_flag));
     } else {
         uint8_t *tmp[kMaxOut];
         for (int o0 = 0; o0 < n_out; o0 += kMaxOut) {
@@ -97,14 +104,13 @@ extern "C" int rsgpu_check_some_shards_noalloc(const uint8_t *rows, int n_in, in
             // groups of kMaxOut so the rows pointer array stays on the stack
             const int no = n_out - o0 < kMaxOut ? n_out - o0 : kMaxOut;
             for (int o = 0; o < no; o++) tmp[o] = scratch + kFlagBytes + pitch * (size_t)(o0 + o);
-            RS_CUDA(launch_gf8_matmul(st, info, rows + (size_t)o0 * n_in, n_in, no, in, tmp, nbytes,
-                                      kModeWrite, d_flag, kTableKernelsOnly));
+            RS_CUDA(launch_gf8_matmul_static(st, info, rows + (size_t)o0 * n_in, n_in, no, in, tmp, nbytes,
+                                             kModeWrite, d_flag));
             const uint8_t one = 1;
             for (int o = 0; o < no; o++) {
                 const uint8_t *src = tmp[o];
                 uint8_t *chk = const_cast<uint8_t *>(to_check[o0 + o]);
-                RS_CUDA(launch_gf8_matmul(st, info, &one, 1, 1, &src, &chk, nbytes, kModeVerify, d_flag,
-                                          kTableKernelsOnly));
+                RS_CUDA(launch_gf8_matmul_static(st, info, &one, 1, 1, &src, &chk, nbytes, kModeVerify, d_flag));
             }
         }
     }

@@ -69,6 +69,8 @@ namespace rsgpu {
 int classic_decode_plan(rsgpu_encoder *enc, const uint8_t *present, int data_only,
                         const uint8_t *required, int n_required, std::vector<uint8_t> &rows,
                         std::vector<int> &out_idx, std::vector<int> &in_idx);
+int decode_idx_plan(rsgpu_encoder *enc, const uint8_t *expect, const uint8_t *has_in, const uint8_t *has_dst,
+                    std::vector<uint8_t> &rows, std::vector<int> &in_shards, std::vector<int> &out_shards);
 // Leopard codec (leopard.cu)
 int leo_create(rsgpu_encoder *enc);
 int leo_encode(rsgpu_encoder *enc, uint8_t *const *shards, size_t size);

@@ -282,14 +282,18 @@ class Encoder:
             raise ErrShardNoData("no shard data")
         if any(p is None or len(p) != size for p in parity) or len(data_shard) != size:
             raise ErrShardSize("shard sizes do not match")
-        self._bind()
-        check(L.lib().rsgpu_encode_idx(self._h, _ptr(data_shard), idx,
-                                       L.ptr_array([_ptr(p) for p in parity]), size))
+        if self._on_device([data_shard] + list(parity)):
+            self._bind()
+            check(L.lib().rsgpu_encode_idx(self._h, _ptr(data_shard), idx,
+                                           L.ptr_array([_ptr(p) for p in parity]), size))
+        else:
+            check(L.lib().rsgpu_encode_idx_host(self._h, _ptr(data_shard), idx,
+                                                L.ptr_array([_ptr(p) for p in parity]), size))
 
     def Update(self, shards, newDatashards):
         """Update (reedsolomon.go:762-853): parity += P * (old ^ new) for every
         data shard with new data; the old data shard is left holding old ^ new,
-        as in the reference.  Device shards only."""
+        as in the reference.  Shards all on the device or all in host memory."""
         if self.codec != RS_CODEC_CLASSIC:
             raise ErrNotSupported("operation not supported")
         if len(shards) != self.TotalShards() or len(newDatashards) != self._k:
@@ -309,12 +313,15 @@ class Encoder:
             raise ErrInvalidInput("invalid input")
         if nsize != size:  # the reference would index past the shorter slices
             raise ErrShardSize("shard sizes do not match")
-        if not dev or not all(_is_device(s) for s in newDatashards if s is not None and len(s)):
-            raise ErrNotSupported("Update takes device shards")
-        self._bind()
         new = [s if (s is not None and len(s)) else None for s in newDatashards]
-        check(L.lib().rsgpu_update(self._h, L.ptr_array([_ptr(s) for s in shards]),
-                                   L.ptr_array([_ptr(s) for s in new]), size))
+        live = [s for s in list(shards) + new if s is not None and len(s)]
+        if self._on_device(live):
+            self._bind()
+            check(L.lib().rsgpu_update(self._h, L.ptr_array([_ptr(s) for s in shards]),
+                                       L.ptr_array([_ptr(s) for s in new]), size))
+        else:
+            check(L.lib().rsgpu_update_host(self._h, L.ptr_array([_ptr(s) for s in shards]),
+                                            L.ptr_array([_ptr(s) for s in new]), size))
 
     def DecodeIdx(self, dst, expectInput, input):
         """DecodeIdx (reedsolomon.go:1464-1617): accumulate this call's inputs
@@ -335,10 +342,12 @@ class Encoder:
             pad = [None] * (self.TotalShards() - 1)
             for i, x in enumerate(input):  # pairs may differ in size: one merge call per pair
                 if x is not None and len(x):
-                    self._device_only([x, dst[i]])
-                    self._bind()
-                    check(lib.rsgpu_decode_idx(self._h, L.ptr_array([_ptr(dst[i])] + pad), None,
-                                               L.ptr_array([_ptr(x)] + pad), len(x)))
+                    if self._on_device([x, dst[i]]):
+                        self._bind()
+                        f = lib.rsgpu_decode_idx
+                    else:
+                        f = lib.rsgpu_decode_idx_host
+                    check(f(self._h, L.ptr_array([_ptr(dst[i])] + pad), None, L.ptr_array([_ptr(x)] + pad), len(x)))
             return
         n = self.TotalShards()
         if len(expectInput) != n or len(dst) != n or len(input) != n:
@@ -363,16 +372,25 @@ class Encoder:
         live = [x for x in list(dst) + list(input) if x is not None and len(x)]
         if not live:
             return
-        self._device_only(live)
-        self._bind()
-        check(lib.rsgpu_decode_idx(self._h, L.ptr_array([_ptr(d) for d in dst]),
-                                   L.u8_array([1 if e else 0 for e in expectInput]),
-                                   L.ptr_array([_ptr(x) for x in input]), size))
+        if self._on_device(live):
+            self._bind()
+            f = lib.rsgpu_decode_idx
+        else:
+            f = lib.rsgpu_decode_idx_host
+        check(f(self._h, L.ptr_array([_ptr(d) for d in dst]), L.u8_array([1 if e else 0 for e in expectInput]),
+                L.ptr_array([_ptr(x) for x in input]), size))
 
     @staticmethod
-    def _device_only(tensors):
-        if not all(_is_device(t) for t in tensors):
-            raise ErrNotSupported("takes device shards")
+    def _on_device(tensors):
+        """True when every tensor is on the device, False when every one is in
+        host memory (the *_host entry points move the bytes); mixed sets are
+        refused."""
+        dev = [_is_device(t) for t in tensors]
+        if all(dev):
+            return True
+        if not any(dev):
+            return False
+        raise ErrNotSupported("shards must be all on the device or all in host memory")
 
     def Split(self, data):
         """Split (reedsolomon.go:1803-1856; leopard.go:320-370) of a 1-D uint8
@@ -448,11 +466,13 @@ class Encoder:
 
     def Verify(self, shards):
         size, dev = self._prep(shards, nilok=False)
-        if not dev:
-            raise ErrNotSupported("Verify takes device shards")
-        self._bind()
         ok = ctypes.c_int()
-        check(L.lib().rsgpu_verify(self._h, L.ptr_array([_ptr(s) for s in shards]), size, ctypes.byref(ok)))
+        if self._on_device(shards):
+            self._bind()
+            check(L.lib().rsgpu_verify(self._h, L.ptr_array([_ptr(s) for s in shards]), size, ctypes.byref(ok)))
+        else:
+            check(L.lib().rsgpu_verify_host(self._h, L.ptr_array([_ptr(s) for s in shards]), size,
+                                            ctypes.byref(ok)))
         return bool(ok.value)
 
     def _reconstruct(self, shards, data_only, required=None):
@@ -507,16 +527,19 @@ class Encoder:
 
     def _reconstruct_host(self, shards, present, want, size, data_only, required):
         """Host buffers: missing outputs are allocated as pinned CPU tensors, PCIe copies run inside."""
-        if required is not None:
-            raise ErrNotSupported("ReconstructSome takes device shards")
         n = self.TotalShards()
         outs = list(shards)
         for i in range(n):
             if want[i]:
                 outs[i] = torch.empty(size, dtype=torch.uint8, pin_memory=True)
         written = (ctypes.c_uint8 * n)()
-        check(L.lib().rsgpu_reconstruct_host(self._h, L.ptr_array([_ptr(s) for s in outs]),
-                                             L.u8_array(present), size, int(data_only), written))
+        ptrs = L.ptr_array([_ptr(s) for s in outs])
+        if required is not None:
+            check(L.lib().rsgpu_reconstruct_some_host(self._h, ptrs, L.u8_array(present),
+                                                      L.u8_array([1 if r else 0 for r in required]),
+                                                      len(required), size, written))
+        else:
+            check(L.lib().rsgpu_reconstruct_host(self._h, ptrs, L.u8_array(present), size, int(data_only), written))
         for i in range(n):
             if written[i]:
                 shards[i] = outs[i]

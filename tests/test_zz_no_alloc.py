@@ -102,3 +102,39 @@ def test_noalloc_runs_table_kernels_only():
         finally:
             lib.rsgpu_force_variant(-1)
     assert lib.rsgpu_xornet_sync() == before
+
+
+def test_noalloc_allocates_nothing_after_first_call():
+    """Once the first call has set a device up, further calls of every shape
+    (tails, 16 outputs, more than 32 inputs) leave the device's free memory
+    exactly as it was: nothing is allocated and no code is loaded."""
+    lib = L.lib()
+    rng = np.random.default_rng(91)
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    calls = []
+    for k, p, size in [(10, 4, (1 << 20) + 16), (5, 3, 1000), (40, 6, 65536), (3, 1, 64), (32, 16, 4096),
+                       (17, 3, 12345), (64, 2, 100000)]:
+        rows = rng.integers(0, 256, (p, k), dtype=np.uint8)
+        data = [rng.integers(0, 256, size, dtype=np.uint8) for _ in range(k)]
+        par = [np.zeros(size, np.uint8) for _ in range(p)]
+        O.code_some_shards(rows, data, par)
+        ins = [torch.from_numpy(d).cuda() for d in data]
+        chk = [torch.from_numpy(x).cuda() for x in par]
+        calls.append((rows, k, p, ins, chk, L.ptr_array([t.data_ptr() for t in ins]),
+                      L.ptr_array([t.data_ptr() for t in chk]), size))
+
+    def run(c):
+        rows, k, p, _, _, pi, pc, size = c
+        ok = ctypes.c_int(-1)
+        assert lib.rsgpu_check_some_shards_noalloc(rows.ctypes.data, k, p, pi, pc, size, stream,
+                                                   ctypes.byref(ok)) == 0, lib.rsgpu_last_error()
+        return ok.value
+
+    assert run(calls[0]) == 1  # set-up call of this test (the device may already be set up)
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    for _ in range(2):
+        for c in calls:
+            assert run(c) == 1
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free_before
