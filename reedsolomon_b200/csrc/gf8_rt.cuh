@@ -4,9 +4,10 @@
 // c*x is the XOR of the bits a of x for which bit b of c*2^a is set (the 8x8
 // bit matrices of the reference's GFNI path, genGFNIMatrix, galois.go:
 // 1004-1016).  On bit-planes (bit a of 32 bytes in one 32-bit word) a product
-// is therefore a fixed XOR pattern of whole words.  The run-time generated XOR network (xornet.cpp)
-// bakes one matrix's coefficients into straight-line code and needs an NVRTC
-// compile per matrix; this kernel is compiled once, ahead of time:
+// is therefore a fixed XOR pattern of whole words.  The run-time generated
+// XOR network (xornet.cpp) bakes one matrix's coefficients into straight-line
+// code and needs an NVRTC compile per matrix; this kernel is compiled once,
+// ahead of time:
 //
 //   * all 256 "accumulate c*x" bodies exist in the binary, one per constant,
 //     each a straight line of at most eight LOP3s;
@@ -23,16 +24,21 @@
 //
 // Register arrays cannot be indexed by a run-time input number, and inlining
 // the 256 bodies once per (output, input) pair makes the code, and ptxas's
-// time (quadratic in the copies), explode.  So a warp's inputs are staged raw in
-// a ring of 1 KiB slots in shared memory with cp.async: each lane owns its
+// time (quadratic in the copies), explode.  So a warp's inputs are staged raw
+// in a ring of 1 KiB slots in shared memory with cp.async: each lane owns its
 // own 16-byte slots (no synchronisation, no bank conflicts), the input loop
 // stays rolled, and the kernel holds exactly four copies of the bodies (one
-// per accumulated output).  The next chunk's inputs are copied into the slots as
-// this chunk consumes them, so loads overlap the arithmetic.
+// per accumulated output).  The next chunk's inputs are copied into the
+// slots as this chunk consumes them, so loads overlap the arithmetic.
 //
-// Any decode matrix (Reconstruct, ReconstructData, ReconstructSome, DecodeIdx)
-// therefore runs the bit-sliced path on first sight, with no compile and no
-// module load.
+// Any matrix (a decode matrix of Reconstruct, ReconstructData, ReconstructSome,
+// DecodeIdx, or a batched job's) runs this bit-sliced path with no compile and
+// no module load.  Measured on B200 it is slower than the nibble-table kernel
+// except for single-output tiles (RS(10,4) x 64 MiB encode: 0.232 ms against
+// 0.204 ms; 10+1: 0.150 against 0.193 ms): each indirect jump costs about
+// eight instructions of dispatch and an instruction-fetch redirect (warps
+// wait on instruction fetch for ~17 % of their cycles), so it runs where the
+// autotuner picks it, not by default.
 #pragma once
 
 #include <cstdint>

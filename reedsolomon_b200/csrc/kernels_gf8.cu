@@ -276,13 +276,15 @@ int choose_variant(int n_in, int n_out, int mode, size_t nbytes) {
     // Untuned default from 256 KiB per shard: the generated XOR network when
     // NVRTC is present (faster than every table kernel at 16 MiB and above in
     // all measured geometries, and at 1 MiB with enough SMs covered); while a
-    // new matrix's network compiles, and without NVRTC, the bit-sliced kernel
-    // with run-time coefficients runs instead.  Below that size the unrolled
-    // table kernel with the most resident warps that does not spill (up to 4
-    // outputs: 4 CTAs per SM when writing, 3 when the outputs are also read,
-    // which holds them in registers; 2 for 5-8 outputs); input counts without
-    // a specialisation fall back to kVariantPrmt.
-    if (nbytes >= kXornetDefaultMin) return xornet_available() ? kVariantXorNet : kVariantBitslice;
+    // new matrix's network compiles, the table kernel below runs instead.
+    // Otherwise the unrolled table kernel with the most resident warps that
+    // does not spill (up to 4 outputs: 4 CTAs per SM when writing, 3 when the
+    // outputs are also read, which holds them in registers; 2 for 5-8
+    // outputs); input counts without a specialisation fall back to
+    // kVariantPrmt.  The bit-sliced run-time-coefficient kernel (variant 8)
+    // is slower than the table kernel for every measured geometry but
+    // single-output ones, so it runs only where the tuner picked it.
+    if (nbytes >= kXornetDefaultMin && xornet_available()) return kVariantXorNet;
     return table_variant(n_out, mode);
 }
 
@@ -319,14 +321,12 @@ cudaError_t launch_gf8_tile(cudaStream_t st, const DeviceInfo &dev, const GfMatA
     long long done = 0;
     if (variant == kVariantXorNet || variant == kVariantBitslice) {
         // Whole 1 KiB chunks through the generated network (compiled on the
-        // spot when forced, else in the background) or, when that is not
-        // ready or not asked for, through the bit-sliced run-time-coefficient
-        // kernel; the tail through the default table kernel.
-        cudaError_t e = cudaSuccess;
-        if (variant == kVariantXorNet)
-            e = xornet_launch(st, dev, a, mode, forced_variant() == kVariantXorNet, &done);
-        if (e != cudaSuccess) return e;
-        if (done == 0) e = launch_bitslice(st, dev, a, mode, &done);
+        // spot when forced, else in the background; while it is not ready the
+        // default table kernel covers everything) or through the bit-sliced
+        // run-time-coefficient kernel; the tail through the table kernel.
+        cudaError_t e = variant == kVariantXorNet
+                            ? xornet_launch(st, dev, a, mode, forced_variant() == kVariantXorNet, &done)
+                            : launch_bitslice(st, dev, a, mode, &done);
         if (e != cudaSuccess) return e;
         variant = table_variant(a.n_out, mode);
         if (done == a.nbytes) return cudaGetLastError();
