@@ -148,6 +148,29 @@ class Context:
         check(L.lib().rsgpu_ctx_set_stream(self.handle, ctypes.c_void_p(s)))
 
 
+class _DeviceBlock:
+    """One device allocation of rsgpu_alloc_shards, freed with rsgpu_free."""
+
+    def __init__(self, ctx, ptr):
+        self.ctx, self.ptr = ctx, ptr
+
+    def __del__(self):
+        try:
+            L.lib().rsgpu_free(self.ctx.handle, ctypes.c_void_p(self.ptr))
+        except Exception:
+            pass
+
+
+class _ShardView:
+    """A shard of a _DeviceBlock exposed through __cuda_array_interface__ (the
+    tensor made from it keeps this object, and so the block, alive)."""
+
+    def __init__(self, block, ptr, n):
+        self._block = block
+        self.__cuda_array_interface__ = {"shape": (int(n),), "typestr": "|u1", "data": (int(ptr), False),
+                                         "version": 3, "strides": None}
+
+
 def _is_device(t):
     return isinstance(t, torch.Tensor) and t.is_cuda
 
@@ -234,11 +257,18 @@ class Encoder:
         return m
 
     def AllocAligned(self, each):
-        """TotalShards device shards of `each` bytes, 64-byte aligned views of one allocation."""
-        pitch = (each + 63) // 64 * 64
-        buf = torch.empty(pitch * self.TotalShards() + 64, dtype=torch.uint8, device="cuda:%d" % self.ctx.device)
-        base = (-buf.data_ptr()) % 64
-        return [buf[base + i * pitch: base + i * pitch + each] for i in range(self.TotalShards())]
+        """AllocAligned (unsafe.go:19-43): TotalShards device shards of `each`
+        bytes carved from one allocation made by rsgpu_alloc_shards, each
+        starting on a 64-byte boundary.  The shards are uint8 CUDA tensors;
+        the allocation is freed when the last of them is released."""
+        if self.ctx is None:
+            raise ErrNoDevice("encoder has no device context")
+        n = self.TotalShards()
+        ptrs = (ctypes.c_void_p * n)()
+        check(L.lib().rsgpu_alloc_shards(self.ctx.handle, n, int(each), ptrs))
+        block = _DeviceBlock(self.ctx, ptrs[0])
+        dev = torch.device("cuda", self.ctx.device)
+        return [torch.as_tensor(_ShardView(block, ptrs[i], each), device=dev) for i in range(n)]
 
     # --- helpers
     def _prep(self, shards, nilok):
