@@ -417,6 +417,7 @@ struct Cache {
 
 void worker_loop();
 Cache &cache();
+void drain_at_exit();
 
 // Starts a compile worker when queued work has no free one, up to a quarter
 // of the host threads (1..4).  Workers never exit (the queue and the cache
@@ -424,6 +425,12 @@ Cache &cache();
 void spawn_workers_locked(Cache &c) {
     const int cap = std::max(1, std::min(4, (int)std::thread::hardware_concurrency() / 4));
     if (!c.queue.empty() && c.workers < cap && c.busy == c.workers) {
+        // Before the first worker starts: drain at exit through atexit.  NVRTC
+        // is loaded (dlopen) after this library, so its static destructors
+        // run before this library's; a handler registered now runs before
+        // them, while no worker may still be inside NVRTC.
+        static std::once_flag registered;
+        std::call_once(registered, [] { std::atexit(drain_at_exit); });
         std::thread(worker_loop).detach();
         c.workers++;
     }
@@ -582,18 +589,20 @@ void worker_loop() {
     }
 }
 
-// At exit (or library unload) queued compiles are dropped and a compile in
-// progress is waited for (bounded), so no worker is inside NVRTC while the
-// process tears down.
+// At exit (atexit, registered when the first worker starts; and again at
+// library unload) queued compiles are dropped and a compile in progress is
+// waited for (bounded), so no worker is inside NVRTC while the process
+// tears down.
+void drain_at_exit() {
+    Cache &c = cache();
+    std::unique_lock<std::mutex> lk(c.mu);
+    for (auto &q : c.queue) q.second->state = Entry::kFailed;
+    c.queue.clear();
+    c.idle.notify_all();  // waiters for an empty queue
+    c.idle.wait_for(lk, std::chrono::seconds(30), [&] { return c.busy == 0; });
+}
 struct DrainAtExit {
-    ~DrainAtExit() {
-        Cache &c = cache();
-        std::unique_lock<std::mutex> lk(c.mu);
-        for (auto &q : c.queue) q.second->state = Entry::kFailed;
-        c.queue.clear();
-        c.idle.notify_all();  // waiters for an empty queue
-        c.idle.wait_for(lk, std::chrono::seconds(30), [&] { return c.busy == 0; });
-    }
+    ~DrainAtExit() { drain_at_exit(); }
 } g_drain_at_exit;
 
 Key make_key(const GfMatArgs &a, int mode) {

@@ -59,3 +59,19 @@ def test_queued_compiles_survive_fork(tmp_path):
         raise
     assert p.returncode == 0, out + err
     assert "child ok=1" in out and "child_status=0" in out
+
+
+@pytest.mark.skipif(shutil.which("g++") is None or not os.path.isdir(CUDA_INC) or not _nvrtc(),
+                    reason="needs g++, CUDA headers and libnvrtc")
+def test_exit_with_compiles_in_flight(tmp_path):
+    """A process that exits while background compiles run exits cleanly
+    (the workers are drained before NVRTC tears itself down)."""
+    rs.lib()
+    exe = tmp_path / "exit_queued"
+    r = subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(PKG, "csrc"), "-I", os.path.join(ROOT, "include"),
+                        "-I", CUDA_INC, os.path.join(HERE, "xornet_exit_queued.cpp"), "-o", str(exe),
+                        "-L", PKG, "-lrsgpu", "-Wl,-rpath," + PKG, "-lpthread"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
+    for _ in range(3):
+        r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0 and "queued" in r.stdout, (r.returncode, r.stderr[-2000:])
