@@ -404,6 +404,15 @@ struct Entry {
     cudaLibrary_t lib = nullptr;
     cudaKernel_t kern = nullptr;
     int blocks_per_sm[64][5] = {};  // [device ordinal][log2 warps per CTA], 0 = not queried
+    // Eviction bookkeeping (all under the cache lock): the cache clock at the
+    // last lookup; launches between their lookup and the event recorded
+    // behind them; events (device, event) recorded behind launches that may
+    // still run, one per launch; and whether a launch was captured into a
+    // graph (then the library is never unloaded).
+    uint64_t last_use = 0;
+    int launching = 0;
+    std::vector<std::pair<int, cudaEvent_t>> pending;
+    bool pinned = false;
 };
 
 struct Cache {
@@ -413,7 +422,35 @@ struct Cache {
     std::deque<std::pair<Key, std::shared_ptr<Entry>>> queue;
     int workers = 0;
     int busy = 0;
+    uint64_t clock = 0;
+    std::map<Key, int> uses;  // launches of matrices not compiled yet (bounded)
+    std::vector<cudaEvent_t> free_events[64];  // per device, completed and reusable
 };
+
+// A matrix is compiled (in the background) once this many launches have
+// asked for it: one-off matrices (a decode matrix seen once) are not worth a
+// compile of 0.2-5 s and a module.  RSGPU_XORNET_MIN_USES overrides it (1:
+// compile on first sight).
+int min_uses() {
+    static const int n = [] {
+        const char *e = getenv("RSGPU_XORNET_MIN_USES");
+        const int v = e ? atoi(e) : 2;
+        return v < 1 ? 1 : v;
+    }();
+    return n;
+}
+constexpr size_t kUsesCap = 16384;  // matrices counted before the counts are reset
+
+// Entries kept (kXornetCacheCap; RSGPU_XORNET_CACHE_CAP overrides it): past
+// it, the least recently used idle entry is evicted and its library unloaded.
+size_t cache_cap() {
+    static const size_t n = [] {
+        const char *e = getenv("RSGPU_XORNET_CACHE_CAP");
+        const long v = e ? atol(e) : kXornetCacheCap;
+        return (size_t)(v < 1 ? 1 : v);
+    }();
+    return n;
+}
 
 void worker_loop();
 Cache &cache();
@@ -616,24 +653,86 @@ Key make_key(const GfMatArgs &a, int mode) {
     return k;
 }
 
+// Unloads evicted entries: waits (per device) for the event recorded after
+// each one's last launch, then unloads its library.  Called without the lock.
+void unload(std::vector<std::shared_ptr<Entry>> &victims) {
+    for (auto &v : victims) {
+        for (auto &pe : v->pending) {
+            cudaEventSynchronize(pe.second);
+            cudaEventDestroy(pe.second);
+        }
+        v->pending.clear();
+        if (v->lib) cudaLibraryUnload(v->lib);
+    }
+    victims.clear();
+}
+
+// An event for a launch on device d: a pooled one, or a new one.  Events
+// behind this entry's earlier launches that have completed go back to the
+// pool first.  Called with the lock.
+cudaEvent_t launch_event_locked(Cache &c, Entry &e, int d) {
+    for (size_t i = 0; i < e.pending.size();) {
+        if (cudaEventQuery(e.pending[i].second) == cudaSuccess) {
+            c.free_events[e.pending[i].first].push_back(e.pending[i].second);
+            e.pending[i] = e.pending.back();
+            e.pending.pop_back();
+        } else {
+            i++;
+        }
+    }
+    cudaEvent_t ev = nullptr;
+    if (!c.free_events[d].empty()) {
+        ev = c.free_events[d].back();
+        c.free_events[d].pop_back();
+    } else if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+        return nullptr;
+    }
+    return ev;
+}
+
+// Makes room for one entry when the cache is full: evicts the least recently
+// used final entry that no launch is using and no graph holds.  False when
+// every entry is busy, queued, compiling or pinned.  Called with the lock.
+bool evict_one_locked(Cache &c, std::vector<std::shared_ptr<Entry>> &victims) {
+    auto best = c.map.end();
+    for (auto it = c.map.begin(); it != c.map.end(); ++it) {
+        const Entry &e = *it->second;
+        if (!e.final_state() || e.launching > 0 || e.pinned) continue;
+        if (best == c.map.end() || e.last_use < best->second->last_use) best = it;
+    }
+    if (best == c.map.end()) return false;
+    victims.push_back(best->second);
+    c.map.erase(best);
+    return true;
+}
+
 // The compiled entry for a's coefficients: compiles now when `sync`, else
-// queues a background compile and returns null until it is ready.
-std::shared_ptr<Entry> lookup(const GfMatArgs &a, int mode, bool sync) {
+// queues a background compile (once the matrix has been asked for
+// min_uses() times) and returns null until it is ready.  `launch`: the caller
+// launches it, and releases it with launch_done() after recording its event.
+std::shared_ptr<Entry> lookup(const GfMatArgs &a, int mode, bool sync, bool launch = false) {
     if (!nvrtc().ok) return nullptr;
     Cache &c = cache();
     Key key = make_key(a, mode);
     std::shared_ptr<Entry> e;
+    std::vector<std::shared_ptr<Entry>> victims;
     {
         std::unique_lock<std::mutex> lk(c.mu);
         auto it = c.map.find(key);
         if (it != c.map.end()) {
             e = it->second;
-            if (e->state == Entry::kCompiled) return e;
+            e->last_use = ++c.clock;
+            if (e->state == Entry::kCompiled) {
+                if (launch) e->launching++;
+                return e;
+            }
             if (e->state == Entry::kFailed || !sync) return nullptr;
             if (e->state == Entry::kCompiling) {
                 // someone else is compiling this entry: wait for them
                 c.idle.wait(lk, [&] { return e->final_state(); });
-                return e->state == Entry::kCompiled ? e : nullptr;
+                if (e->state != Entry::kCompiled) return nullptr;
+                if (launch) e->launching++;
+                return e;
             }
             // still queued: take it out of the queue and compile it here
             for (auto q = c.queue.begin(); q != c.queue.end(); ++q)
@@ -641,25 +740,34 @@ std::shared_ptr<Entry> lookup(const GfMatArgs &a, int mode, bool sync) {
                     c.queue.erase(q);
                     break;
                 }
-        } else if (c.map.size() >= (size_t)kXornetCacheCap) {
-            return nullptr;
         } else {
+            if (!sync) {
+                if (c.uses.size() >= kUsesCap) c.uses.clear();
+                if (++c.uses[key] < min_uses()) return nullptr;
+                c.uses.erase(key);
+            }
+            if (c.map.size() >= cache_cap() && !evict_one_locked(c, victims)) return nullptr;
             e = std::make_shared<Entry>();
+            e->last_use = ++c.clock;
             c.map.emplace(key, e);
             if (!sync) {
                 c.queue.emplace_back(key, e);
                 spawn_workers_locked(c);
                 c.cv.notify_one();
+                lk.unlock();
+                unload(victims);
                 return nullptr;
             }
         }
         e->state = Entry::kCompiling;
     }
+    unload(victims);
     std::vector<char> bin = build_kernel(key);
     {
         std::lock_guard<std::mutex> lk(c.mu);
         e->cubin = std::move(bin);
         e->state = e->cubin.empty() ? Entry::kFailed : Entry::kCompiled;
+        if (launch && e->state == Entry::kCompiled) e->launching++;
     }
     c.idle.notify_all();
     return e->state == Entry::kCompiled ? e : nullptr;
@@ -703,8 +811,9 @@ cudaError_t xornet_launch(cudaStream_t st, const DeviceInfo &dev, const GfMatArg
         if (reinterpret_cast<uintptr_t>(a.in[i]) & 15u) return cudaSuccess;
     for (int o = 0; o < a.n_out; o++)
         if (reinterpret_cast<uintptr_t>(a.out[o]) & 15u) return cudaSuccess;
-    std::shared_ptr<Entry> e = lookup(a, mode, sync);
+    std::shared_ptr<Entry> e = lookup(a, mode, sync, /*launch=*/true);
     if (!e) return cudaSuccess;
+    Cache &c = cache();
     // Warps per CTA: the compiled maximum, halved while that would leave SMs
     // without work (1 MiB shards are 1024 warp steps: 4-warp CTAs spread
     // them over every SM where 16-warp CTAs would fill 64).
@@ -712,23 +821,33 @@ cudaError_t xornet_launch(cudaStream_t st, const DeviceInfo &dev, const GfMatArg
     while ((32 << (lw + 1)) <= xornet_threads(a.n_out)) lw++;
     while (lw > 0 && nchunk < (long long)dev.sm_count << lw) lw--;
     const int threads = 32 << lw;
+    const int d = dev.device & 63;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) cap = cudaStreamCaptureStatusInvalidated;
+    const bool capturing = cap != cudaStreamCaptureStatusNone;
     cudaKernel_t kern;
     int nb;
     {
-        std::lock_guard<std::mutex> lk(cache().mu);
+        std::lock_guard<std::mutex> lk(c.mu);
         if (!e->lib) {
             // No module loading inside a stream capture: the table kernel
             // stands in until an uncaptured launch has loaded this one.
-            cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
-            if (cudaStreamIsCapturing(st, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone)
+            if (capturing) {
+                e->launching--;
                 return cudaSuccess;
+            }
             cudaError_t rc = cudaLibraryLoadData(&e->lib, e->cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
-            if (rc != cudaSuccess) return rc;
-            rc = cudaLibraryGetKernel(&e->kern, e->lib, "rs_xornet");
-            if (rc != cudaSuccess) return rc;
+            if (rc == cudaSuccess) rc = cudaLibraryGetKernel(&e->kern, e->lib, "rs_xornet");
+            if (rc != cudaSuccess) {
+                e->launching--;
+                return rc;
+            }
         }
+        // A graph holding this kernel may be replayed at any time: never
+        // unload it once a launch has been captured.
+        if (capturing) e->pinned = true;
         kern = e->kern;
-        int &slot = e->blocks_per_sm[dev.device & 63][lw];
+        int &slot = e->blocks_per_sm[d][lw];
         if (slot == 0) {
             int q = 0;
             if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&q, (const void *)kern, threads, 0) !=
@@ -750,6 +869,22 @@ cudaError_t xornet_launch(cudaStream_t st, const DeviceInfo &dev, const GfMatArg
     const int grid = (int)std::max(1LL, std::min(want, (long long)dev.sm_count * nb));
     void *args[] = {&x};
     cudaError_t rc = cudaLaunchKernel((const void *)kern, dim3(grid), dim3(threads), args, 0, st);
+    {
+        // the event an eviction waits for before unloading the library
+        std::lock_guard<std::mutex> lk(c.mu);
+        if (rc == cudaSuccess && !capturing) {
+            cudaEvent_t ev = launch_event_locked(c, *e, d);
+            if (!ev) {
+                e->pinned = true;  // nothing to wait on: keep the library for good
+            } else if (cudaEventRecord(ev, st) != cudaSuccess) {
+                cudaEventDestroy(ev);
+                e->pinned = true;
+            } else {
+                e->pending.emplace_back(d, ev);
+            }
+        }
+        e->launching--;
+    }
     if (rc == cudaSuccess) *bytes_done = nchunk * kXornetChunk;
     return rc;
 }

@@ -11,7 +11,7 @@ namespace rsgpu {
 
 constexpr int kXornetChunk = 1024;   // bytes of every shard per warp step
 constexpr int kXornetMaxOut = 16;
-constexpr int kXornetCacheCap = 512; // compiled matrices kept per process
+constexpr int kXornetCacheCap = 512; // matrices kept per process; the least recently used idle one is evicted
 constexpr size_t kXornetDefaultMin = 256 << 10;  // untuned default from this many bytes per shard
 
 // Threads per CTA of a tile's kernel: 512 (a 128-register cap, 16 warps per

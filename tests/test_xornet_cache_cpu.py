@@ -75,3 +75,20 @@ def test_exit_with_compiles_in_flight(tmp_path):
     for _ in range(3):
         r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
         assert r.returncode == 0 and "queued" in r.stdout, (r.returncode, r.stderr[-2000:])
+
+
+@pytest.mark.skipif(shutil.which("g++") is None or not os.path.isdir(CUDA_INC) or not _nvrtc(),
+                    reason="needs g++, CUDA headers and libnvrtc")
+def test_compile_after_two_uses_and_lru_eviction(tmp_path):
+    """A one-off matrix is not compiled; a second request queues it; at the
+    cache's capacity new compiles evict the least recently used entries."""
+    rs.lib()
+    exe = tmp_path / "policy"
+    r = subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(PKG, "csrc"), "-I", os.path.join(ROOT, "include"),
+                        "-I", CUDA_INC, os.path.join(HERE, "xornet_policy.cpp"), "-o", str(exe),
+                        "-L", PKG, "-lrsgpu", "-Wl,-rpath," + PKG, "-lpthread"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
+    env = dict(os.environ, RSGPU_XORNET_CACHE_CAP="3")
+    env.pop("RSGPU_XORNET_MIN_USES", None)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300, env=env)
+    assert r.returncode == 0, r.stdout + r.stderr

@@ -175,7 +175,7 @@ def test_record_and_force_variant_arguments():
     are refused; a recorded choice can be removed again."""
     lib = rs.lib()
     n = lib.rsgpu_num_variants()
-    assert n == 8
+    assert n == 9
     assert lib.rsgpu_record_variant(10, 4, 1 << 20, 0, 7) == 0
     assert lib.rsgpu_record_variant(10, 4, 1 << 20, 0, -1) == 0
     for args in [(0, 4, 1 << 20, 0, 7), (33, 4, 1 << 20, 0, 7), (10, 17, 1 << 20, 0, 7), (10, 4, 0, 0, 7),

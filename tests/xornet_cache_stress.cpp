@@ -26,7 +26,8 @@ int main() {
             for (int s = 0; s < 12; s++) {
                 GfMatArgs a = mk(100 * t + s, 6, 3);
                 long long done = -1;
-                xornet_launch(nullptr, dev, a, 0, false, &done);
+                xornet_launch(nullptr, dev, a, 0, false, &done);  // counted
+                xornet_launch(nullptr, dev, a, 0, false, &done);  // queued
             }
         });
     for (int t = 0; t < 3; t++)

@@ -1,5 +1,5 @@
 // Exit with XOR-network compiles still queued and running (no GPU needed):
-// queues 40 matrices through xornet_launch (which returns before any CUDA
+// queues 40 matrices (each asked for twice) through xornet_launch (which returns before any CUDA
 // call while a matrix is not compiled) and returns from main at once.  The
 // process must exit cleanly: the compile workers are drained before NVRTC's
 // own teardown.
@@ -20,7 +20,8 @@ int main() {
         for (int o = 0; o < 4; o++)
             for (int i = 0; i < 10; i++) a.coef[o][i] = (uint8_t)((s * 131 + o * 31 + i * 7) | 1);
         long long done = -1;
-        xornet_launch(nullptr, dev, a, 0, false, &done);
+        xornet_launch(nullptr, dev, a, 0, false, &done);  // counted
+        xornet_launch(nullptr, dev, a, 0, false, &done);  // queued
     }
     printf("queued\n");
     return 0;

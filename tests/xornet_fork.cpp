@@ -17,7 +17,9 @@ static GfMatArgs mk(int seed) {
 }
 int main() {
     DeviceInfo dev; dev.sm_count = 148;
-    for (int s = 0; s < 8; s++) { GfMatArgs a = mk(s); long long d; xornet_launch(nullptr, dev, a, 0, false, &d); }
+    // each matrix asked for twice: the second request queues its compile
+    for (int r = 0; r < 2; r++)
+        for (int s = 0; s < 8; s++) { GfMatArgs a = mk(s); long long d; xornet_launch(nullptr, dev, a, 0, false, &d); }
     pid_t pid = fork();
     if (pid == 0) {
         GfMatArgs a = mk(1000);
