@@ -639,7 +639,8 @@ def extra_c1(dev, reps=200):
     present = rs._lib.u8_array([0 if i in lost else 1 for i in range(k + p)])
     # warm-up: two calls of each kind queue their matrices' kernel compiles
     # (variant 7 is the default at this size); finish them before timing
-    keep = [sh[i].clone() for i in lost]
+    rs.encoder.check(lib.rsgpu_encode(enc._h, ptrs, S))
+    keep = [sh[i].clone() for i in lost]  # the originals, parity included
     for _ in range(2):
         rs.encoder.check(lib.rsgpu_encode(enc._h, ptrs, S))
         rs.encoder.check(lib.rsgpu_verify(enc._h, ptrs, S, ctypes.byref(ok)))
