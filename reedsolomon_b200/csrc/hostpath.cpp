@@ -24,8 +24,11 @@ struct Pipeline {
 
     int init(int n_rows, size_t size, size_t align) {
         rows = n_rows;
-        // ~8 chunks per call, at least 1 MiB per row, aligned for Leopard.
+        // ~8 chunks per call, at least 1 MiB per row, aligned for Leopard;
+        // with many rows (Leopard: up to 65536) the ring is held to 1 GiB.
         size_t c = std::max<size_t>(size / 8, (size_t)1 << 20);
+        const size_t budget = ((size_t)1 << 30) / ((size_t)rows * kRing);
+        c = std::min(c, std::max(budget, align));
         c = std::min(c, size);
         c = (c + align - 1) / align * align;
         chunk = std::min(c, size);

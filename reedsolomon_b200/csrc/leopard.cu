@@ -44,7 +44,7 @@ struct LeoState {
     uint16_t *ts16 = nullptr;    // [65535][4][16] nibble tables in fftSkew order (see F16S)
     uint16_t *skew8 = nullptr;   // fftSkew8, 255 entries (widened)
     uint8_t *t8 = nullptr;       // [256][2][16] nibble products
-    uint16_t *fold16 = nullptr;  // W_n of FWHT(log) for n = 2^0..2^11 (see leo_errloc_kernel)
+    uint16_t *fold16 = nullptr;  // W_n of FWHT(log) for n = 2^0..2^16 (see leo_errloc_kernel)
     uint16_t *fold8 = nullptr;   // W_n of FWHT(log8) for n = 2^0..2^8
     ~LeoState() {
         if (device >= 0) {
@@ -787,6 +787,208 @@ __global__ void __launch_bounds__(kLeoDecodeThreads) leo_decode_kernel(const __g
     }
 }
 
+// ---- GF(2^16) geometries past one CTA's shared memory ---------------------
+// Past 2048 shard pointers or 2048 transform rows (the reference allows up
+// to 65536 shards, leopard.go:51-70) the transforms run over a work buffer
+// in HBM, one row per pitch bytes in the reference's chunk layout, in
+// passes.  A pass executes consecutive butterfly layers whose groups fit a
+// set of at most kLeoSetRows rows: a set is rows base + t * d_lo, t < rows,
+// where d_lo is the smallest distance of the pass (upper layers take sets of
+// strided rows, lower layers sets of consecutive rows).  Each CTA loads one
+// set's 64-byte column tile into shared memory, runs the pass's layers on it
+// with multipliers indexed by global row numbers exactly as ifftDIT /
+// fftDIT index them (leopard.go:650-736, :764-873), and writes it back.
+constexpr int kLeoSetRows = 1024;  // 64 KB of shared memory per CTA
+constexpr int kLeoPassThreads = 512;
+constexpr int kLeoMaxLayers = 16;
+
+struct LeoPassArgs {
+    uint8_t *w;       // work rows
+    long long pitch;  // bytes between work rows
+    const uint16_t *skew, *t16;
+    int n_layers;
+    int d_lo;      // row stride inside a set
+    int span;      // global rows one set's butterfly groups cover (set rows * d_lo)
+    int set_rows;  // rows per set
+    int mtrunc;    // butterfly groups starting at or above this row are skipped
+    int skew_off;  // IFFT multiplier offset (-1 decoder, m-1+b*m encoder block b)
+    int fft;       // 1: fftDIT layers, 0: ifftDIT layers
+    int dist[kLeoMaxLayers];   // the layers' global distances, in execution order
+    int radix[kLeoMaxLayers];  // 4 or 2
+};
+
+__global__ void __launch_bounds__(kLeoPassThreads) leo_pass16_kernel(const __grid_constant__ LeoPassArgs a) {
+    extern __shared__ __align__(16) uint8_t sm[];
+    using Q = F16::Q;
+    F16 f;
+    f.t = a.t16;
+    f.skew = a.skew;
+    const long long col = (long long)blockIdx.x * kLeoTile;
+    const unsigned set = blockIdx.y, d_lo = (unsigned)a.d_lo;
+    const unsigned g = set / d_lo, o = set % d_lo;
+    const long long gbase = (long long)g * a.span;  // global start of the set's group
+    const unsigned rows = (unsigned)a.set_rows;
+    auto grow = [&](unsigned t) { return a.w + (gbase + o + (long long)t * d_lo) * a.pitch + col; };
+    for (unsigned v = threadIdx.x; v < rows * F16::kRowParts; v += blockDim.x)
+        F16::row_in(sm + (size_t)(v / F16::kRowParts) * kLeoTile, grow(v / F16::kRowParts), v % F16::kRowParts);
+    __syncthreads();
+    for (int L = 0; L < a.n_layers; L++) {
+        const unsigned dist = (unsigned)a.dist[L], ld = dist / d_lo;  // global and local distance
+        if (a.radix[L] == 4) {
+            const unsigned groups = rows / (4 * ld);
+            for (unsigned it = threadIdx.x; it < ((groups * ld) << F16::kQuadShift); it += blockDim.x) {
+                const unsigned q = it >> F16::kQuadShift, c = it & (F16::kQuads - 1);
+                const unsigned gl = q / ld, i = gl * 4 * ld + q % ld;
+                const long long r = gbase + (long long)gl * 4 * ld * d_lo;  // group start, global
+                if (r >= a.mtrunc) continue;
+                uint8_t *p0 = sm + (size_t)i * kLeoTile;
+                uint8_t *p1 = p0 + (size_t)ld * kLeoTile, *p2 = p1 + (size_t)ld * kLeoTile,
+                        *p3 = p2 + (size_t)ld * kLeoTile;
+                Q x0 = F16::ld(p0, c), x1 = F16::ld(p1, c), x2 = F16::ld(p2, c), x3 = F16::ld(p3, c);
+                const long long iend = r + dist;
+                if (a.fft) {
+                    const uint32_t m01 = a.skew[iend - 1], m02 = a.skew[iend + dist - 1],
+                                   m23 = a.skew[iend + 2 * dist - 1];
+                    fft2(f, x0, x2, m02);
+                    fft2(f, x1, x3, m02);
+                    fft2(f, x0, x1, m01);
+                    fft2(f, x2, x3, m23);
+                } else {
+                    const uint32_t m01 = a.skew[a.skew_off + iend], m02 = a.skew[a.skew_off + iend + dist],
+                                   m23 = a.skew[a.skew_off + iend + 2 * dist];
+                    ifft2(f, x0, x1, m01);
+                    ifft2(f, x2, x3, m23);
+                    ifft2(f, x0, x2, m02);
+                    ifft2(f, x1, x3, m02);
+                }
+                F16::st(p0, c, x0);
+                F16::st(p1, c, x1);
+                F16::st(p2, c, x2);
+                F16::st(p3, c, x3);
+            }
+        } else {
+            // radix 2: the IFFT's top layer (dist = n/2, every pair, multiplier
+            // fftSkew[skew_off + dist]) or the FFT's last (dist = 1, pairs
+            // (r, r+1) below mtrunc, multiplier fftSkew[r])
+            const unsigned groups = rows / (2 * ld);
+            for (unsigned it = threadIdx.x; it < ((groups * ld) << F16::kQuadShift); it += blockDim.x) {
+                const unsigned q = it >> F16::kQuadShift, c = it & (F16::kQuads - 1);
+                const unsigned gl = q / ld, i = gl * 2 * ld + q % ld;
+                const long long r = gbase + (long long)gl * 2 * ld * d_lo;
+                if (a.fft && r >= a.mtrunc) continue;
+                uint8_t *p0 = sm + (size_t)i * kLeoTile, *p1 = p0 + (size_t)ld * kLeoTile;
+                Q x = F16::ld(p0, c), y = F16::ld(p1, c);
+                if (a.fft) fft2(f, x, y, (uint32_t)a.skew[r]);
+                else ifft2(f, x, y, (uint32_t)a.skew[a.skew_off + (long long)dist]);
+                F16::st(p0, c, x);
+                F16::st(p1, c, y);
+            }
+        }
+        __syncthreads();
+    }
+    for (unsigned v = threadIdx.x; v < rows * F16::kRowParts; v += blockDim.x)
+        F16::row_out(grow(v / F16::kRowParts), sm + (size_t)(v / F16::kRowParts) * kLeoTile, v % F16::kRowParts);
+}
+
+// Formal derivative (leopard.go:620-623) on rows [c0, c0 + crows) of the
+// work buffer: row x gains old[x + 2^b] for every b with bit b of x clear and
+// ((x>>b)+1)<<b < n.  Launched for ascending chunks: rows past the chunk are
+// still old, and inside it every read comes before the barrier that precedes
+// the writes.  XOR is bytewise, so the raw layout is used as it is.
+__global__ void __launch_bounds__(kLeoPassThreads) leo_deriv16_chunk_kernel(uint8_t *w, long long pitch, unsigned n,
+                                                                           unsigned c0, unsigned crows) {
+    extern __shared__ __align__(16) uint8_t sm[];  // crows * 64 bytes of new values
+    const long long col = (long long)blockIdx.x * kLeoTile;
+    unsigned lg = 0;
+    while ((2u << lg) <= n) lg++;
+    for (unsigned v = threadIdx.x; v < crows * 4; v += blockDim.x) {
+        const unsigned x = c0 + v / 4, part = v % 4;
+        uint4 acc = reinterpret_cast<const uint4 *>(w + (long long)x * pitch + col)[part];
+        for (unsigned b = 0; b < lg; b++) {
+            if (((x >> b) & 1u) || ((((x >> b) + 1) << b) >= n)) continue;
+            const uint4 y = reinterpret_cast<const uint4 *>(w + (long long)(x + (1u << b)) * pitch + col)[part];
+            acc.x ^= y.x;
+            acc.y ^= y.y;
+            acc.z ^= y.z;
+            acc.w ^= y.w;
+        }
+        reinterpret_cast<uint4 *>(sm)[v] = acc;
+    }
+    __syncthreads();
+    for (unsigned v = threadIdx.x; v < crows * 4; v += blockDim.x)
+        reinterpret_cast<uint4 *>(w + (long long)(c0 + v / 4) * pitch + col)[v % 4] = reinterpret_cast<uint4 *>(sm)[v];
+}
+
+// Work rows [0, rows) <- shards [first, first + cnt) (raw copy), zero past cnt.
+__global__ void leo_rows_in_kernel(uint8_t *w, long long pitch, const uint8_t *const *shard, int first, int cnt,
+                                   int rows, long long vecs_per_row) {
+    const long long total = (long long)rows * vecs_per_row;
+    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < total;
+         v += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(v / vecs_per_row);
+        const long long e = v % vecs_per_row;
+        const uint4 x = r < cnt ? __ldcs(reinterpret_cast<const uint4 *>(shard[first + r]) + e) : make_uint4(0, 0, 0, 0);
+        reinterpret_cast<uint4 *>(w + (long long)r * pitch)[e] = x;
+    }
+}
+
+// Shards [first, first + cnt) <- work rows [0, cnt).
+__global__ void leo_rows_out_kernel(const uint8_t *w, long long pitch, const uint8_t *const *shard, int first,
+                                    int cnt, long long vecs_per_row) {
+    const long long total = (long long)cnt * vecs_per_row;
+    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < total;
+         v += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(v / vecs_per_row);
+        const long long e = v % vecs_per_row;
+        __stcs(reinterpret_cast<uint4 *>(const_cast<uint8_t *>(shard[first + r])) + e,
+               reinterpret_cast<const uint4 *>(w + (long long)r * pitch)[e]);
+    }
+}
+
+// Decoder input (leopard.go:586-605): work row r = received shard times its
+// error locator (parity at rows [0, p), data at [m, m+k)), zero elsewhere.
+__global__ void leo_dec_load16_kernel(uint8_t *w, long long pitch, const uint8_t *const *shard,
+                                      const uint32_t *present, const uint16_t *errloc, const uint16_t *t16,
+                                      const uint16_t *skew, int k, int p, int m, int n, long long quads_per_row) {
+    F16 f;
+    f.t = t16;
+    f.skew = skew;
+    const long long total = (long long)n * quads_per_row;
+    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < total;
+         v += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(v / quads_per_row);
+        const long long qq = v % quads_per_row, chunk = qq / F16::kQuads;
+        const int c = (int)(qq % F16::kQuads);
+        int src = -1;
+        if (r < p) src = k + r;
+        else if (r >= m && r < m + k) src = r - m;
+        F16::Q x = F16::zero();
+        if (src >= 0 && bit(present, src)) x = f.mul(F16::ldg(shard[src] + chunk * kLeoTile, c), errloc[r]);
+        F16::stg(w + (long long)r * pitch + chunk * kLeoTile, c, x);
+    }
+}
+
+// Reveal (leopard.go:636-647): shard i <- work row times (modulus - errloc).
+__global__ void leo_reveal16_kernel(const uint8_t *w, long long pitch, const uint8_t *const *shard,
+                                    const uint32_t *write, const uint16_t *errloc, const uint16_t *t16,
+                                    const uint16_t *skew, int k, int total, int m, long long quads_per_row) {
+    F16 f;
+    f.t = t16;
+    f.skew = skew;
+    const long long all = (long long)total * quads_per_row;
+    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < all;
+         v += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(v / quads_per_row);
+        if (!bit(write, i)) continue;
+        const long long qq = v % quads_per_row, chunk = qq / F16::kQuads;
+        const int c = (int)(qq % F16::kQuads);
+        const unsigned row = i >= k ? (unsigned)(i - k) : (unsigned)i + (unsigned)m;
+        const uint32_t lm = F16::kMod - errloc[row];
+        F16::stg(const_cast<uint8_t *>(shard[i]) + chunk * kLeoTile, c,
+                 f.mul(F16::ldg(w + (long long)row * pitch + chunk * kLeoTile, c), lm));
+    }
+}
+
 // Error locators of an erasure pattern (leopard.go:468-510,
 // leopard8.go:465-513).  The reference puts ones at erased rows (parity rows
 // first, the padding rows p..m-1, data rows at offset m), takes a 2^BITS-point
@@ -836,8 +1038,10 @@ __device__ void wht_shared(uint16_t *v, unsigned n) {
     }
 }
 
+constexpr int kLeoMaxAllShards = 65536;  // leopard.go:51-70
+
 struct LeoErrArgs {
-    uint32_t present[kLeoMaxShards / 32];
+    uint32_t present[kLeoMaxAllShards / 32];
     int k, p, m, n;
     const uint16_t *fold;  // W_n
     uint16_t *out;
@@ -848,7 +1052,7 @@ constexpr int kErrLocThreads = 512;
 template <int BITS>
 __global__ void __launch_bounds__(kErrLocThreads) leo_errloc_kernel(const __grid_constant__ LeoErrArgs a) {
     constexpr uint32_t kMod = (1u << BITS) - 1;
-    __shared__ uint16_t el[kLeoMaxRows];
+    extern __shared__ __align__(16) uint16_t el[];  // n entries (at most 65536: 128 KB)
     const unsigned m = (unsigned)a.m, k = (unsigned)a.k, p = (unsigned)a.p, n = (unsigned)a.n;
     for (unsigned i = threadIdx.x; i < n; i += blockDim.x) {
         uint16_t v = 0;
@@ -935,7 +1139,7 @@ int ensure_tables(rsgpu_encoder *enc) {
     RS_CUDA(cudaMemcpy(st->skew16, f16.skew.data(), 65535 * 2, cudaMemcpyHostToDevice));
     RS_CUDA(cudaMemcpy(st->skew8, f8.skew.data(), 255 * 2, cudaMemcpyHostToDevice));
     {
-        const std::vector<uint16_t> w16 = fold_walsh<16>(f16.walsh, 11), w8 = fold_walsh<8>(f8.walsh, 8);
+        const std::vector<uint16_t> w16 = fold_walsh<16>(f16.walsh, 16), w8 = fold_walsh<8>(f8.walsh, 8);
         RS_CUDA(cudaMalloc(&st->fold16, w16.size() * 2));
         RS_CUDA(cudaMalloc(&st->fold8, w8.size() * 2));
         RS_CUDA(cudaMemcpy(st->fold16, w16.data(), w16.size() * 2, cudaMemcpyHostToDevice));
@@ -989,6 +1193,164 @@ int set_smem(K kern, size_t bytes) {
     return RS_OK;
 }
 
+// ---- GF(2^16) past one CTA: passes over a work buffer in HBM --------------
+
+// The layers of an n-row ifftDIT (ascending radix-4 distances, then one
+// radix-2 layer at n/2 when log2 n is odd) or fftDIT (descending radix-4
+// distances, then one radix-2 layer at distance 1), exactly as
+// ifft_rows / fft_rows run them, grouped into passes whose sets stay within
+// kLeoSetRows rows.
+std::vector<LeoPassArgs> plan_passes(unsigned n, bool fft) {
+    std::vector<std::pair<unsigned, int>> layers;  // (distance, radix)
+    if (!fft) {
+        unsigned dist = 1, dist4 = 4;
+        for (; dist4 <= n; dist = dist4, dist4 <<= 2) layers.push_back({dist, 4});
+        if (dist < n) layers.push_back({dist, 2});
+    } else {
+        unsigned dist4 = n, dist = n >> 2;
+        for (; dist != 0; dist4 = dist, dist >>= 2) layers.push_back({dist, 4});
+        if (dist4 == 2) layers.push_back({1u, 2});
+    }
+    std::vector<LeoPassArgs> passes;
+    for (size_t first = 0; first < layers.size();) {
+        unsigned lo = layers[first].first, span = layers[first].first * layers[first].second;
+        size_t end = first + 1;
+        while (end < layers.size() && end - first < (size_t)kLeoMaxLayers) {
+            const unsigned nlo = std::min(lo, layers[end].first);
+            const unsigned nspan = std::max(span, layers[end].first * (unsigned)layers[end].second);
+            if (nspan / nlo > (unsigned)kLeoSetRows) break;
+            lo = nlo;
+            span = nspan;
+            end++;
+        }
+        LeoPassArgs a;
+        memset(&a, 0, sizeof a);
+        a.n_layers = (int)(end - first);
+        a.d_lo = (int)lo;
+        a.span = (int)span;
+        a.set_rows = (int)(span / lo);
+        a.fft = fft ? 1 : 0;
+        for (size_t L = first; L < end; L++) {
+            a.dist[L - first] = (int)layers[L].first;
+            a.radix[L - first] = layers[L].second;
+        }
+        passes.push_back(a);
+        first = end;
+    }
+    return passes;
+}
+
+// Runs an n-row transform on work rows w (pitch bytes apart, `size` bytes
+// of every row processed).
+int run_passes(const LeoState &L, uint8_t *w, long long pitch, size_t size, unsigned n, bool fft, int mtrunc,
+               int skew_off, cudaStream_t st) {
+    int rc = set_smem(leo_pass16_kernel, (size_t)kLeoSetRows * kLeoTile);  // per device, so on every call
+    if (rc) return rc;
+    for (LeoPassArgs a : plan_passes(n, fft)) {
+        a.w = w;
+        a.pitch = pitch;
+        a.skew = L.skew16;
+        a.t16 = L.t16;
+        a.mtrunc = mtrunc;
+        a.skew_off = skew_off;
+        const dim3 grid((unsigned)(size / kLeoTile), (unsigned)(n / (unsigned)a.set_rows));
+        leo_pass16_kernel<<<grid, kLeoPassThreads, (size_t)a.set_rows * kLeoTile, st>>>(a);
+        RS_CUDA(cudaGetLastError());
+    }
+    return RS_OK;
+}
+
+// Grid of the row-copy / row-map kernels.
+int rows_grid(long long items) { return (int)std::max(1LL, std::min((items + 255) / 256, 148LL * 16)); }
+
+// Stream-ordered scratch from the context pool, freed behind the call's work.
+struct PoolScratch {
+    cudaStream_t st;
+    cudaMemPool_t pool;
+    std::vector<void *> blocks;
+    int get(void **p, size_t bytes) {
+        RS_CUDA(cudaMallocFromPoolAsync(p, bytes ? bytes : 16, pool, st));
+        blocks.push_back(*p);
+        return RS_OK;
+    }
+    ~PoolScratch() {
+        for (void *b : blocks) cudaFreeAsync(b, st);
+    }
+};
+
+// Encode (leopard.go:169-270) for GF(2^16) geometries past one CTA: work rows
+// [0, m) accumulate, [m, 2m) hold each later data block; every block's IFFT
+// and the final FFT run as passes.
+int leo_encode_large(rsgpu_encoder *enc, uint8_t *const *shards, size_t size, cudaStream_t st) {
+    const int k = enc->k, p = enc->p, total = enc->total;
+    const unsigned m = ceil_pow2((unsigned)p);
+    const LeoState &L = *enc->leo;
+    PoolScratch sc{st, enc->ctx->pool, {}};
+    const uint8_t **dptr = nullptr;
+    uint8_t *w = nullptr;
+    int rc = sc.get((void **)&dptr, sizeof(void *) * (size_t)total);
+    if (!rc) rc = sc.get((void **)&w, (size_t)2 * m * size);
+    if (rc) return rc;
+    RS_CUDA(cudaMemcpyAsync(dptr, shards, sizeof(void *) * (size_t)total, cudaMemcpyHostToDevice, st));
+    const long long pitch = (long long)size, vecs = (long long)(size / 16);
+    uint8_t *acc = w, *tmp = w + (size_t)m * size;
+    for (int b = 0; b * (int)m < k; b++) {
+        const int start = b * (int)m, cnt = std::min((int)m, k - start);
+        uint8_t *dst = b == 0 ? acc : tmp;
+        leo_rows_in_kernel<<<rows_grid((long long)m * vecs), 256, 0, st>>>(dst, pitch, dptr, start, cnt, (int)m, vecs);
+        RS_CUDA(cudaGetLastError());
+        rc = run_passes(L, dst, pitch, size, m, false, cnt, (int)m - 1 + b * (int)m, st);
+        if (rc) return rc;
+        if (b > 0) RS_CUDA(launch_xor(st, enc->ctx->info, tmp, acc, (size_t)m * size));
+    }
+    rc = run_passes(L, acc, pitch, size, m, true, p, 0, st);
+    if (rc) return rc;
+    leo_rows_out_kernel<<<rows_grid((long long)p * vecs), 256, 0, st>>>(acc, pitch, dptr, k, p, vecs);
+    RS_CUDA(cudaGetLastError());
+    return RS_OK;
+}
+
+// Decode (leopard.go:582-647) for GF(2^16) geometries past one CTA, given the
+// first n error locators on the device.
+int leo_decode_large(rsgpu_encoder *enc, uint8_t *const *shards, const std::vector<uint32_t> &present,
+                     const std::vector<uint32_t> &write, const uint16_t *d_el, unsigned m, unsigned n,
+                     int input_count, size_t size, cudaStream_t st) {
+    const int k = enc->k, p = enc->p, total = enc->total;
+    const LeoState &L = *enc->leo;
+    PoolScratch sc{st, enc->ctx->pool, {}};
+    const uint8_t **dptr = nullptr;
+    uint32_t *dpres = nullptr, *dwrite = nullptr;
+    uint8_t *w = nullptr;
+    int rc = sc.get((void **)&dptr, sizeof(void *) * (size_t)total);
+    if (!rc) rc = sc.get((void **)&dpres, present.size() * 4);
+    if (!rc) rc = sc.get((void **)&dwrite, write.size() * 4);
+    if (!rc) rc = sc.get((void **)&w, (size_t)n * size);
+    if (rc) return rc;
+    RS_CUDA(cudaMemcpyAsync(dptr, shards, sizeof(void *) * (size_t)total, cudaMemcpyHostToDevice, st));
+    RS_CUDA(cudaMemcpyAsync(dpres, present.data(), present.size() * 4, cudaMemcpyHostToDevice, st));
+    RS_CUDA(cudaMemcpyAsync(dwrite, write.data(), write.size() * 4, cudaMemcpyHostToDevice, st));
+    const long long pitch = (long long)size, quads = (long long)(size / kLeoTile) * F16::kQuads;
+    leo_dec_load16_kernel<<<rows_grid((long long)n * quads), 256, 0, st>>>(w, pitch, dptr, dpres, d_el, L.t16,
+                                                                           L.skew16, k, p, (int)m, (int)n, quads);
+    RS_CUDA(cudaGetLastError());
+    rc = run_passes(L, w, pitch, size, n, false, input_count, -1, st);
+    if (rc) return rc;
+    const unsigned crows = std::min(n, (unsigned)kLeoSetRows);
+    rc = set_smem(leo_deriv16_chunk_kernel, (size_t)kLeoSetRows * kLeoTile);
+    if (rc) return rc;
+    for (unsigned c0 = 0; c0 < n; c0 += crows) {
+        leo_deriv16_chunk_kernel<<<(unsigned)(size / kLeoTile), kLeoPassThreads, (size_t)crows * kLeoTile, st>>>(
+            w, pitch, n, c0, crows);
+        RS_CUDA(cudaGetLastError());
+    }
+    rc = run_passes(L, w, pitch, size, n, true, (int)m + k, 0, st);
+    if (rc) return rc;
+    leo_reveal16_kernel<<<rows_grid((long long)total * quads), 256, 0, st>>>(w, pitch, dptr, dwrite, d_el, L.t16,
+                                                                             L.skew16, k, total, (int)m, quads);
+    RS_CUDA(cudaGetLastError());
+    return RS_OK;
+}
+
 }  // namespace
 
 int leo_create(rsgpu_encoder *enc) {
@@ -1002,16 +1364,18 @@ int leo_create(rsgpu_encoder *enc) {
 int leo_encode_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, size_t size, cudaStream_t st) {
     if (size % 64) return RS_ERR_INVALID_SHARD_SIZE;
     const unsigned m = ceil_pow2((unsigned)enc->p);
-    if (enc->total > kLeoMaxShards || 2 * m > kLeoMaxRows) {
-        set_error("leopard encode: geometry exceeds the shared-memory transform (k+p <= 2048, 2*ceilPow2(p) <= 2048)");
-        return RS_ERR_NOT_SUPPORTED;
-    }
     if (!shards_aligned(shards, enc->total)) {
         set_error("leopard encode: shard buffers must be 16-byte aligned");
         return RS_ERR_NOT_SUPPORTED;
     }
+    const bool fits_cta = enc->total <= kLeoMaxShards && 2 * m <= kLeoMaxRows;
+    if (!fits_cta && !is16(enc)) {  // not reachable by a valid GF(2^8) geometry (k+p <= 256)
+        set_error("leopard encode: geometry exceeds the shared-memory transform");
+        return RS_ERR_NOT_SUPPORTED;
+    }
     int rc = ensure_tables(enc);
     if (rc) return rc;
+    if (!fits_cta) return leo_encode_large(enc, shards, size, st ? st : enc->ctx->stream);
     LeoEncArgs a;
     memset(&a, 0, sizeof a);
     for (int i = 0; i < enc->total; i++) a.shard[i] = shards[i];
@@ -1077,32 +1441,30 @@ int leo_reconstruct_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, const ui
     bool nothing = false;
     int rc = decode_checks(enc, present, size, recover_all, &nothing);
     if (rc || nothing) return rc;
-    const int k = enc->k, p = enc->p;
+    const int k = enc->k, p = enc->p, total = enc->total;
     const unsigned m = ceil_pow2((unsigned)p), n = ceil_pow2(m + (unsigned)k);
-    if (enc->total > kLeoMaxShards || n > kLeoMaxRows) {
-        set_error("leopard decode: geometry exceeds the shared-memory transform (ceilPow2(ceilPow2(p)+k) <= 2048)");
+    const bool g16 = is16(enc);
+    const bool fits_cta = total <= kLeoMaxShards && n <= (unsigned)kLeoMaxRows;
+    if (!fits_cta && !g16) {  // not reachable by a valid GF(2^8) geometry (k+p <= 256)
+        set_error("leopard decode: geometry exceeds the shared-memory transform");
         return RS_ERR_NOT_SUPPORTED;
     }
-    if (!shards_aligned(shards, enc->total)) {
+    if (!shards_aligned(shards, total)) {
         set_error("leopard reconstruct: shard buffers must be 16-byte aligned");
         return RS_ERR_NOT_SUPPORTED;
     }
     rc = ensure_tables(enc);
     if (rc) return rc;
-    const bool g16 = is16(enc);
-    static_assert(sizeof(LeoDecArgs) < 32000, "kernel parameter limit");
-    auto a = std::unique_ptr<LeoDecArgs>(new LeoDecArgs());
-    memset(a.get(), 0, sizeof *a);
     int input_count = p;
     for (int i = 0; i < k; i++)
         if (present[i]) input_count = (int)m + i + 1;
-    const int end = recover_all ? enc->total : k;
-    for (int i = 0; i < enc->total; i++) {
-        a->shard[i] = shards[i];
-        if (present[i]) a->present[i >> 5] |= 1u << (i & 31);
+    const int end = recover_all ? total : k;
+    std::vector<uint32_t> pres((total + 31) / 32, 0), write((total + 31) / 32, 0);
+    for (int i = 0; i < total; i++) {
+        if (present[i]) pres[i >> 5] |= 1u << (i & 31);
         else if (i < end) {
             if (!shards[i]) return RS_ERR_INVALID_INPUT;
-            a->write[i >> 5] |= 1u << (i & 31);
+            write[i >> 5] |= 1u << (i & 31);
         }
     }
     if (!st) st = enc->ctx->stream;
@@ -1114,11 +1476,10 @@ int leo_reconstruct_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, const ui
         enc->errlocs->device = enc->ctx->device;
     }
     LeoErrLocCache &cache = *enc->errlocs;
-    const std::vector<uint32_t> key(a->present, a->present + (enc->total + 31) / 32);
     uint16_t *d_el = nullptr;
     {
         std::lock_guard<std::mutex> lk(cache.mu);
-        auto it = cache.map.find(key);
+        auto it = cache.map.find(pres);
         if (it != cache.map.end()) {
             d_el = it->second.d;
             RS_CUDA(cudaStreamWaitEvent(st, it->second.ready, 0));
@@ -1128,30 +1489,34 @@ int leo_reconstruct_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, const ui
     if (!d_el) {
         RS_CUDA(cudaMallocFromPoolAsync((void **)&d_el, (size_t)n * sizeof(uint16_t), enc->ctx->pool, st));
         owned = true;
-    }
-    LeoErrArgs ea;
-    memset(&ea, 0, sizeof ea);
-    memcpy(ea.present, a->present, sizeof ea.present);
-    ea.k = k;
-    ea.p = p;
-    ea.m = (int)m;
-    ea.n = (int)n;
-    ea.out = d_el;
-    ea.fold = (g16 ? enc->leo->fold16 : enc->leo->fold8) + n;
-    if (owned) {
-        if (g16) leo_errloc_kernel<16><<<1, kErrLocThreads, 0, st>>>(ea);
-        else leo_errloc_kernel<8><<<1, kErrLocThreads, 0, st>>>(ea);
+        auto ea = std::unique_ptr<LeoErrArgs>(new LeoErrArgs());
+        memset(ea.get(), 0, sizeof *ea);
+        memcpy(ea->present, pres.data(), pres.size() * 4);
+        ea->k = k;
+        ea->p = p;
+        ea->m = (int)m;
+        ea->n = (int)n;
+        ea->out = d_el;
+        ea->fold = (g16 ? enc->leo->fold16 : enc->leo->fold8) + n;
+        const size_t el_smem = (size_t)n * sizeof(uint16_t);
+        if (g16) rc = set_smem(leo_errloc_kernel<16>, el_smem > (48u << 10) ? el_smem : (48u << 10));
+        if (rc) {
+            cudaFreeAsync(d_el, st);
+            return rc;
+        }
+        if (g16) leo_errloc_kernel<16><<<1, kErrLocThreads, el_smem, st>>>(*ea);
+        else leo_errloc_kernel<8><<<1, kErrLocThreads, el_smem, st>>>(*ea);
         rc = cuda_status(cudaGetLastError(), "leo_errloc_kernel");
         if (rc) {
             cudaFreeAsync(d_el, st);
             return rc;
         }
         std::lock_guard<std::mutex> lk(cache.mu);
-        if (cache.map.size() < kErrLocCacheCap && !cache.map.count(key)) {
+        if (cache.map.size() < kErrLocCacheCap && !cache.map.count(pres)) {
             cudaEvent_t ev = nullptr;
             if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess) {
                 if (cudaEventRecord(ev, st) == cudaSuccess) {
-                    cache.map[key] = LeoErrLocCache::Entry{d_el, ev};
+                    cache.map[pres] = LeoErrLocCache::Entry{d_el, ev};
                     owned = false;
                 } else {
                     cudaEventDestroy(ev);
@@ -1159,6 +1524,17 @@ int leo_reconstruct_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, const ui
             }
         }
     }
+    if (!fits_cta) {
+        rc = leo_decode_large(enc, shards, pres, write, d_el, m, n, input_count, size, st);
+        if (owned) cudaFreeAsync(d_el, st);
+        return rc;
+    }
+    static_assert(sizeof(LeoDecArgs) < 32000, "kernel parameter limit");
+    auto a = std::unique_ptr<LeoDecArgs>(new LeoDecArgs());
+    memset(a.get(), 0, sizeof *a);
+    for (int i = 0; i < total; i++) a->shard[i] = shards[i];
+    memcpy(a->present, pres.data(), pres.size() * 4);
+    memcpy(a->write, write.data(), write.size() * 4);
     a->errloc = d_el;
     a->k = k;
     a->p = p;
