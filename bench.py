@@ -401,6 +401,12 @@ def extra_batch(dev, n_stripes, seed=77, sample=16, cpu_seconds=3.0):
     ie, ir = enc_b.info(), rec_b.info()
     res = {"stripes": n_stripes, "encode_jobs": ie["jobs"], "reconstruct_jobs": ir["jobs"],
            "bytes_per_pass": ie["bytes"] + ir["bytes"]}
+    # the persistent launch's tile size and CTAs per SM, chosen by the autotuner
+    tuned = {}
+    for name, b in (("encode", enc_b), ("reconstruct", rec_b)):
+        tile, ctas, ms = b.autotune()
+        tuned[name] = {"tile_bytes": tile, "ctas_per_sm": ctas, "ms": round(ms, 3)}
+    res["autotuned"] = tuned
     stream = torch.cuda.current_stream(dev)
     for mode in ("persistent", "graph", "per_stripe"):
         enc_b.run(mode)

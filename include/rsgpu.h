@@ -272,6 +272,12 @@ int rsgpu_batch_results(rsgpu_batch *batch, int *ok, int n);
 int rsgpu_batch_info(rsgpu_batch *batch, int *n_stripes, int *n_jobs, long long *n_tiles, double *bytes);
 /* Tile size of the persistent launch in bytes (multiple of 4096; 0 = default). */
 int rsgpu_batch_set_tile(rsgpu_batch *batch, int tile_bytes);
+/* Autotuner of the persistent launch (no counterpart in the reference): runs
+ * the batch's own jobs (reps timed runs per shape; every run rewrites the
+ * same outputs) for tile sizes 4-64 KiB and 2-4 persistent CTAs per SM, keeps
+ * the fastest shape for later runs and reports it (any out pointer may be
+ * NULL). */
+int rsgpu_batch_autotune(rsgpu_batch *batch, int reps, int *tile_bytes, int *ctas_per_sm, float *ms);
 
 /* ---- StreamEncoder (streaming.go:23-700) -----------------------------------
  * Block-wise Encode / Verify / Reconstruct over caller callbacks (the

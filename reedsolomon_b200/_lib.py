@@ -136,6 +136,7 @@ SIGNATURES = {
     "rsgpu_batch_results": (c_int, [c_voidp, c_intp, c_int]),
     "rsgpu_batch_info": (c_int, [c_voidp, c_intp, c_intp, ctypes.POINTER(ctypes.c_longlong),
                                  ctypes.POINTER(ctypes.c_double)]),
+    "rsgpu_batch_autotune": (c_int, [c_voidp, c_int, c_intp, c_intp, ctypes.POINTER(ctypes.c_float)]),
     "rsgpu_batch_set_tile": (c_int, [c_voidp, c_int]),
     "rsgpu_server_create": (c_int, [c_voidp, c_size, c_size, c_int, c_int, ctypes.POINTER(c_voidp)]),
     "rsgpu_server_submit": (c_int, [c_voidp, c_voidp, ctypes.POINTER(ctypes.c_uint64)]),

@@ -159,6 +159,7 @@ struct rsgpu_batch {
     std::vector<BatchJob> irregular;     // misaligned / ragged jobs: per-job launches
     int n_stripes = 0;
     int tile_bytes = 0;                  // 0: default
+    int ctas_per_sm = 0;                 // persistent CTAs per SM; 0: default
     bool dirty = true;
     // device state
     BatchJob *d_jobs = nullptr;
@@ -265,7 +266,7 @@ void plan_tiles(rsgpu_batch *b, std::vector<long long> &cta_first) {
             resident = 1;
         resident_by_dev[dev].store(resident, std::memory_order_relaxed);
     }
-    const int per_sm = std::min(resident, kBatchBlocksPerSm);
+    const int per_sm = std::min(resident, b->ctas_per_sm > 0 ? b->ctas_per_sm : kBatchBlocksPerSm);
     const int grid = std::max(1, (int)std::min<long long>(t, (long long)b->ctx->info.sm_count * per_sm));
     b->grid = grid;
     cta_first.assign(grid + 1, t);
@@ -381,6 +382,55 @@ int rsgpu_batch_set_tile(rsgpu_batch *b, int tile_bytes) {
     if (!b || tile_bytes < 0 || (tile_bytes % 4096) != 0) return RS_ERR_INVALID_INPUT;
     b->tile_bytes = tile_bytes;
     b->dirty = true;
+    return RS_OK;
+}
+
+int rsgpu_batch_autotune(rsgpu_batch *b, int reps, int *tile_out, int *ctas_out, float *ms_out) {
+    RS_TRACE("rsgpu_batch_autotune");
+    if (!b) return RS_ERR_INVALID_INPUT;
+    std::lock_guard<std::recursive_mutex> lk(b->ctx->mu);
+    if (b->jobs.empty()) return RS_ERR_SHARD_NO_DATA;
+    if (reps < 1) reps = 2;
+    cudaStream_t st = b->ctx->stream;
+    cudaEvent_t e0, e1;
+    RS_CUDA(cudaEventCreate(&e0));
+    RS_CUDA(cudaEventCreate(&e1));
+    static const int kTiles[] = {4096, 8192, 16384, 32768, 65536};
+    static const int kCtas[] = {2, 3, 4};
+    float best = 1e30f;
+    int best_tile = kDefaultTile, best_ctas = kBatchBlocksPerSm, rc = RS_OK;
+    for (int ctas : kCtas)
+        for (int tile : kTiles) {
+            b->tile_bytes = tile;
+            b->ctas_per_sm = ctas;
+            b->dirty = true;
+            rc = batch_run_on(b, RS_BATCH_PERSISTENT, st);  // plans, uploads and warms this shape
+            if (rc) break;
+            float ms = 0;
+            if (cudaEventRecord(e0, st) != cudaSuccess) { rc = RS_ERR_CUDA; break; }
+            for (int r = 0; r < reps && !rc; r++) rc = batch_run_on(b, RS_BATCH_PERSISTENT, st);
+            if (rc) break;
+            if (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+                rc = RS_ERR_CUDA;
+                break;
+            }
+            ms /= reps;
+            if (ms < best) {
+                best = ms;
+                best_tile = tile;
+                best_ctas = ctas;
+            }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    b->tile_bytes = best_tile;
+    b->ctas_per_sm = best_ctas;
+    b->dirty = true;
+    if (rc) return rc;
+    if (tile_out) *tile_out = best_tile;
+    if (ctas_out) *ctas_out = best_ctas;
+    if (ms_out) *ms_out = best;
     return RS_OK;
 }
 

@@ -908,6 +908,16 @@ class Batch:
     def set_tile(self, tile_bytes):
         check(L.lib().rsgpu_batch_set_tile(self._h, int(tile_bytes)))
 
+    def autotune(self, reps=2):
+        """Times the persistent launch over this batch's jobs for several
+        tile sizes and CTAs per SM and keeps the fastest: (tile bytes, CTAs
+        per SM, ms per run)."""
+        self.ctx.bind_current_stream()
+        tile, ctas, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
+        check(L.lib().rsgpu_batch_autotune(self._h, int(reps), ctypes.byref(tile), ctypes.byref(ctas),
+                                           ctypes.byref(ms)))
+        return tile.value, ctas.value, ms.value
+
     def run(self, mode="persistent", wait=True):
         self.ctx.bind_current_stream()
         f = L.lib().rsgpu_batch_run if wait else L.lib().rsgpu_batch_run_async

@@ -100,3 +100,25 @@ def test_batch_data_only_and_errors():
         k, p, size, ref, lost = stripes[0]
         sh = [torch.from_numpy(a).cuda() for a in ref]
         rs.Batch().add_reconstruct(k, p, sh, [0] * (p + 1) + [1] * (k - 1))
+
+
+def test_batch_autotune_keeps_outputs_exact():
+    """The autotuner runs the batch's own jobs for each candidate shape; the
+    chosen shape is kept, and outputs stay equal to the oracle's."""
+    stripes = make_stripes(24, 23)
+    enc_b = rs.Batch()
+    dev = []
+    for (k, p, size, ref, lost) in stripes:
+        sh = [torch.from_numpy(a).cuda() if i < k else torch.zeros(size, dtype=torch.uint8, device="cuda")
+              for i, a in enumerate(ref)]
+        dev.append(sh)
+        enc_b.add_encode(k, p, sh)
+    tile, ctas, ms = enc_b.autotune(reps=1)
+    assert tile in (4096, 8192, 16384, 32768, 65536) and ctas in (2, 3, 4) and ms > 0
+    for (k, p, size, ref, lost), sh in zip(stripes, dev):
+        for i in range(k, k + p):
+            sh[i].zero_()
+    enc_b.run("persistent")
+    for (k, p, size, ref, lost), sh in zip(stripes, dev):
+        for i in range(k, k + p):
+            assert np.array_equal(sh[i].cpu().numpy(), ref[i]), (k, p, size, i)
