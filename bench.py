@@ -506,6 +506,21 @@ def leopard_cpu(gf, k, p, shards, lost, seconds):
     return len(ranges), k * S * ne / ee / 1e9, k * S * nr / er / 1e9
 
 
+def lookup_ceiling_gproducts(dev, lookups_per_product):
+    """SMs x max SM clock x 32 shared-memory lookups per clock, per product
+    (billions of symbol products per second); None without NVML."""
+    import torch
+    try:
+        import pynvml
+        pynvml.nvmlInit()
+        h = pynvml.nvmlDeviceGetHandleByIndex(dev.index or 0)
+        mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+    except Exception:
+        return None
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    return sms * mhz * 1e6 * 32 / lookups_per_product / 1e9
+
+
 def extra_leopard(dev, cpu_seconds=2.0):
     """C4: Leopard GF(2^16) 1000+200 x 64 KiB and GF(2^8) 192+56 x 256 KiB
     encode / reconstruct (p random erasures), device-resident.  Rebuilt shards
@@ -567,6 +582,9 @@ def extra_leopard(dev, cpu_seconds=2.0):
         enc_products = ((k + m - 1) // m + 1) * (m // 2) * lg(m) * syms
         dec_products = 2 * (n // 2) * lg(n) * syms
         threads, ce, cr = leopard_cpu(gf, k, p, [s.cpu().numpy() for s in sh], lost, cpu_seconds)
+        # lookup ceiling: one shared-memory lookup per lane per clock per SM,
+        # 4 lookups per GF(2^16) product (nibble tables), 2 per GF(2^8)
+        ceiling = lookup_ceiling_gproducts(dev, 4 if gf == 16 else 2)
         out[name] = {"encode_ms": round(ms_e, 4), "encode_data_GBps": round(k * size / (ms_e / 1e3) / 1e9, 1),
                      "encode_frac_of_hbm": round((k + p) * size / (ms_e / 1e3) / 1e9 / peaks()[0], 4),
                      "encode_Gproducts_per_s": round(enc_products / (ms_e / 1e3) / 1e9, 1),
@@ -574,6 +592,11 @@ def extra_leopard(dev, cpu_seconds=2.0):
                      "reconstruct_data_GBps": round(k * size / (ms_r / 1e3) / 1e9, 1),
                      "reconstruct_frac_of_hbm": round((k + p) * size / (ms_r / 1e3) / 1e9 / peaks()[0], 4),
                      "reconstruct_Gproducts_per_s": round(dec_products / (ms_r / 1e3) / 1e9, 1),
+                     "lookup_ceiling_Gproducts_per_s": round(ceiling, 1) if ceiling else None,
+                     "encode_frac_of_lookup_ceiling": round(enc_products / (ms_e / 1e3) / 1e9 / ceiling, 3)
+                     if ceiling else None,
+                     "reconstruct_frac_of_lookup_ceiling": round(dec_products / (ms_r / 1e3) / 1e9 / ceiling, 3)
+                     if ceiling else None,
                      "bit_exact": bit_exact,
                      "cpu_baseline": {"encode_data_GBps": round(ce, 3), "reconstruct_data_GBps": round(cr, 3),
                                       "cores": threads, "kind": "port",
