@@ -56,7 +56,7 @@ def parse():
                     help="shard size; the headline workload is 64 MiB")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the secondary measurements (verify, reconstruct, batch, leopard)")
-    ap.add_argument("--extras", default="c1,verify,reconstruct,progressive,stream,batch,leopard,serving",
+    ap.add_argument("--extras", default="c1,verify,reconstruct,progressive,stream,batch,leopard,leopard_large,serving",
                     help="comma list of secondary measurements to run")
     ap.add_argument("--batch-stripes", type=int, default=4096)
     ap.add_argument("--variant", type=int, default=-1,
@@ -604,6 +604,57 @@ def extra_leopard(dev, cpu_seconds=2.0):
     return out
 
 
+def extra_leopard_large(dev, reps=2):
+    """Leopard GF(2^16) past one CTA (multi-pass transforms over an HBM work
+    buffer): 3000+1000 x 64 KiB, 8192+4096 x 64 KiB and the reference's
+    maximum 32768+32768 x 16 KiB; encode, then p random erasures rebuilt
+    (reconstruct) and compared with the original bytes."""
+    import torch
+    import reedsolomon_b200 as rs
+    out = {}
+    lib = rs.lib()
+    stream = torch.cuda.current_stream(dev)
+    for k, p, size in ((3000, 1000, 65536), (8192, 4096, 65536), (32768, 32768, 16384)):
+        g = torch.Generator(device=dev).manual_seed(k + p)
+        pool = torch.empty((k + p) * size, dtype=torch.uint8, device=dev)
+        pool[:k * size].copy_(torch.randint(0, 256, (k * size,), dtype=torch.uint8, device=dev, generator=g))
+        sh = [pool[i * size:(i + 1) * size] for i in range(k + p)]
+        enc = rs.New(k, p, rs.WithLeopardGF16())
+        enc.ctx.bind_current_stream()
+        ptrs = rs._lib.ptr_array([s.data_ptr() for s in sh])
+        rs.encoder.check(lib.rsgpu_encode_async(enc._h, ptrs, size))
+        a, b = _ev(), _ev()
+        a.record(stream)
+        for _ in range(reps):
+            rs.encoder.check(lib.rsgpu_encode_async(enc._h, ptrs, size))
+        b.record(stream)
+        b.synchronize()
+        ms_e = a.elapsed_time(b) / reps
+        rng = np.random.default_rng(k)
+        lost = sorted(rng.choice(k + p, size=p, replace=False).tolist())
+        orig = pool.clone()
+        present = rs._lib.u8_array([0 if i in lost else 1 for i in range(k + p)])
+        rs.encoder.check(lib.rsgpu_reconstruct_async(enc._h, ptrs, present, size, 0))  # warm (error locators)
+        for i in lost:
+            sh[i].zero_()
+        a, b = _ev(), _ev()
+        a.record(stream)
+        for _ in range(reps):
+            rs.encoder.check(lib.rsgpu_reconstruct_async(enc._h, ptrs, present, size, 0))
+        b.record(stream)
+        b.synchronize()
+        ms_r = a.elapsed_time(b) / reps
+        ok = bool(torch.equal(pool, orig))
+        assert ok, "large Leopard reconstruct differs from the original bytes"
+        out["%d+%dx%dKiB" % (k, p, size >> 10)] = {
+            "encode_ms": round(ms_e, 3), "encode_data_GBps": round(k * size / (ms_e / 1e3) / 1e9, 1),
+            "reconstruct_ms": round(ms_r, 3), "erasures": p,
+            "reconstruct_data_GBps": round(k * size / (ms_r / 1e3) / 1e9, 1), "bit_exact": ok}
+        del pool, orig, sh
+        torch.cuda.empty_cache()
+    return out
+
+
 def extra_progressive(enc, shards, S, reps=5):
     """Update of 2 of the 10 data shards and a 4-erasure DecodeIdx fed in two
     progressive calls, on the RS(10,4) x 64 MiB stripe (copies, so the
@@ -1006,6 +1057,8 @@ def run_ours(args):
             extras["batch"] = extra_batch(dev, args.batch_stripes)
         if "leopard" in want:
             extras["leopard"] = extra_leopard(dev)
+        if "leopard_large" in want:
+            extras["leopard_large"] = extra_leopard_large(dev)
         if "progressive" in want:
             extras["progressive"] = extra_progressive(enc, shards, S)
         if "stream" in want:
