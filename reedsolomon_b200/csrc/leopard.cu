@@ -810,6 +810,7 @@ struct LeoPassArgs {
     int d_lo;      // row stride inside a set
     int span;      // global rows one set's butterfly groups cover (set rows * d_lo)
     int set_rows;  // rows per set
+    int sets;      // sets per CTA (they fill up to kLeoSetRows rows of shared memory)
     int mtrunc;    // butterfly groups starting at or above this row are skipped
     int skew_off;  // IFFT multiplier offset (-1 decoder, m-1+b*m encoder block b)
     int fft;       // 1: fftDIT layers, 0: ifftDIT layers
@@ -824,22 +825,29 @@ __global__ void __launch_bounds__(kLeoPassThreads) leo_pass16_kernel(const __gri
     f.t = a.t16;
     f.skew = a.skew;
     const long long col = (long long)blockIdx.x * kLeoTile;
-    const unsigned set = blockIdx.y, d_lo = (unsigned)a.d_lo;
-    const unsigned g = set / d_lo, o = set % d_lo;
-    const long long gbase = (long long)g * a.span;  // global start of the set's group
-    const unsigned rows = (unsigned)a.set_rows;
-    auto grow = [&](unsigned t) { return a.w + (gbase + o + (long long)t * d_lo) * a.pitch + col; };
-    for (unsigned v = threadIdx.x; v < rows * F16::kRowParts; v += blockDim.x)
+    const unsigned d_lo = (unsigned)a.d_lo, rows = (unsigned)a.set_rows, nsets = (unsigned)a.sets;
+    const unsigned set0 = blockIdx.y * nsets;
+    // local row lr = s * rows + t is row t of set set0 + s: global row
+    // g * span + o + t * d_lo with g, o the set's group and offset
+    auto gstart = [&](unsigned s) { return (long long)((set0 + s) / d_lo) * a.span; };
+    auto grow = [&](unsigned lr) {
+        const unsigned s = lr / rows, t = lr % rows;
+        return a.w + (gstart(s) + (set0 + s) % d_lo + (long long)t * d_lo) * a.pitch + col;
+    };
+    const unsigned all = nsets * rows;
+    for (unsigned v = threadIdx.x; v < all * F16::kRowParts; v += blockDim.x)
         F16::row_in(sm + (size_t)(v / F16::kRowParts) * kLeoTile, grow(v / F16::kRowParts), v % F16::kRowParts);
     __syncthreads();
     for (int L = 0; L < a.n_layers; L++) {
         const unsigned dist = (unsigned)a.dist[L], ld = dist / d_lo;  // global and local distance
-        if (a.radix[L] == 4) {
-            const unsigned groups = rows / (4 * ld);
-            for (unsigned it = threadIdx.x; it < ((groups * ld) << F16::kQuadShift); it += blockDim.x) {
-                const unsigned q = it >> F16::kQuadShift, c = it & (F16::kQuads - 1);
-                const unsigned gl = q / ld, i = gl * 4 * ld + q % ld;
-                const long long r = gbase + (long long)gl * 4 * ld * d_lo;  // group start, global
+        const unsigned span_l = (unsigned)a.radix[L] * ld;           // local rows of one butterfly group
+        const unsigned per_set = (rows / span_l) * ld;               // butterfly positions per set
+        for (unsigned it = threadIdx.x; it < ((nsets * per_set) << F16::kQuadShift); it += blockDim.x) {
+            const unsigned q = it >> F16::kQuadShift, c = it & (F16::kQuads - 1);
+            const unsigned s = q / per_set, qs = q % per_set;
+            const unsigned gl = qs / ld, i = s * rows + gl * span_l + qs % ld;
+            const long long r = gstart(s) + (long long)gl * span_l * d_lo;  // group start, global
+            if (a.radix[L] == 4) {
                 if (r >= a.mtrunc) continue;
                 uint8_t *p0 = sm + (size_t)i * kLeoTile;
                 uint8_t *p1 = p0 + (size_t)ld * kLeoTile, *p2 = p1 + (size_t)ld * kLeoTile,
@@ -865,16 +873,10 @@ __global__ void __launch_bounds__(kLeoPassThreads) leo_pass16_kernel(const __gri
                 F16::st(p1, c, x1);
                 F16::st(p2, c, x2);
                 F16::st(p3, c, x3);
-            }
-        } else {
-            // radix 2: the IFFT's top layer (dist = n/2, every pair, multiplier
-            // fftSkew[skew_off + dist]) or the FFT's last (dist = 1, pairs
-            // (r, r+1) below mtrunc, multiplier fftSkew[r])
-            const unsigned groups = rows / (2 * ld);
-            for (unsigned it = threadIdx.x; it < ((groups * ld) << F16::kQuadShift); it += blockDim.x) {
-                const unsigned q = it >> F16::kQuadShift, c = it & (F16::kQuads - 1);
-                const unsigned gl = q / ld, i = gl * 2 * ld + q % ld;
-                const long long r = gbase + (long long)gl * 2 * ld * d_lo;
+            } else {
+                // radix 2: the IFFT's top layer (dist = n/2, every pair,
+                // multiplier fftSkew[skew_off + dist]) or the FFT's last
+                // (dist = 1, pairs (r, r+1) below mtrunc, multiplier fftSkew[r])
                 if (a.fft && r >= a.mtrunc) continue;
                 uint8_t *p0 = sm + (size_t)i * kLeoTile, *p1 = p0 + (size_t)ld * kLeoTile;
                 Q x = F16::ld(p0, c), y = F16::ld(p1, c);
@@ -886,7 +888,7 @@ __global__ void __launch_bounds__(kLeoPassThreads) leo_pass16_kernel(const __gri
         }
         __syncthreads();
     }
-    for (unsigned v = threadIdx.x; v < rows * F16::kRowParts; v += blockDim.x)
+    for (unsigned v = threadIdx.x; v < all * F16::kRowParts; v += blockDim.x)
         F16::row_out(grow(v / F16::kRowParts), sm + (size_t)(v / F16::kRowParts) * kLeoTile, v % F16::kRowParts);
 }
 
@@ -1253,8 +1255,10 @@ int run_passes(const LeoState &L, uint8_t *w, long long pitch, size_t size, unsi
         a.t16 = L.t16;
         a.mtrunc = mtrunc;
         a.skew_off = skew_off;
-        const dim3 grid((unsigned)(size / kLeoTile), (unsigned)(n / (unsigned)a.set_rows));
-        leo_pass16_kernel<<<grid, kLeoPassThreads, (size_t)a.set_rows * kLeoTile, st>>>(a);
+        const unsigned nsets = n / (unsigned)a.set_rows;
+        a.sets = (int)std::min(nsets, (unsigned)kLeoSetRows / (unsigned)a.set_rows);
+        const dim3 grid((unsigned)(size / kLeoTile), nsets / (unsigned)a.sets);
+        leo_pass16_kernel<<<grid, kLeoPassThreads, (size_t)a.sets * a.set_rows * kLeoTile, st>>>(a);
         RS_CUDA(cudaGetLastError());
     }
     return RS_OK;
