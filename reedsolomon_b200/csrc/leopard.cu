@@ -31,6 +31,7 @@
 namespace rsgpu {
 
 constexpr int kLeoThreads = 256;        // encode CTAs (2m rows of shared memory each)
+constexpr int kLeoEncThreadsMax = 512;  // staged GF(2^16) encode: 2m threads up to this
 constexpr int kLeoDecodeThreads = 1024; // decode CTAs hold up to 128 KB: one per SM, so 32 warps
 constexpr int kLeoTile = 64;          // bytes of every row owned by one CTA
 constexpr int kLeoMaxShards = 2048;   // shard pointers carried in kernel parameters
@@ -42,6 +43,7 @@ struct LeoState {
     uint16_t *skew16 = nullptr;  // fftSkew, 65535 entries
     uint16_t *t16 = nullptr;     // [65536][kT16Stride] split product tables (see F16)
     uint16_t *ts16 = nullptr;    // [65535][4][16] nibble tables in fftSkew order (see F16S)
+    uint16_t *tw16 = nullptr;    // [16384][128] wide tables of fftSkew indices 4j+3 (see F16W)
     uint16_t *skew8 = nullptr;   // fftSkew8, 255 entries (widened)
     uint8_t *t8 = nullptr;       // [256][2][16] nibble products
     uint16_t *fold16 = nullptr;  // W_n of FWHT(log) for n = 2^0..2^16 (see leo_errloc_kernel)
@@ -51,6 +53,7 @@ struct LeoState {
             cudaFree(skew16);
             cudaFree(t16);
             cudaFree(ts16);
+            cudaFree(tw16);
             cudaFree(skew8);
             cudaFree(t8);
             cudaFree(fold16);
@@ -106,6 +109,7 @@ struct LeoEncArgs {
     const uint16_t *skew;
     const uint16_t *t16;
     const uint16_t *ts16;
+    const uint16_t *tw16;
     const uint8_t *t8;
 };
 
@@ -113,6 +117,7 @@ struct LeoDecArgs {
     const uint8_t *shard[kLeoMaxShards];
     const uint16_t *errloc;               // the first n error locators (device)
     const uint16_t *ts16;
+    const uint16_t *tw16;
     uint32_t present[kLeoMaxShards / 32];
     uint32_t write[kLeoMaxShards / 32];   // missing shards to reveal
     int k, p, m, n, input_count;
@@ -263,14 +268,17 @@ struct F8 {
 // A transform over fftSkew indices [lo, lo + count) stages, for slot
 // s = index - lo, the four 16-entry nibble product tables of skew[index]
 // (all zero when skew[index] is the modulus, which the reference treats as a
-// zero product, so no test is needed).  Slot s lives in the 256-byte block
-// s >> 1 at half (s & 1) * 128, and its nibble table q at 32-byte position
-// (q + (s >> 2)) & 3 of that half: the four groups a warp covers in the first
+// zero product, so no test is needed).  Slot s lives at position t: t = s,
+// or, when the transform never reads slots s = 3 (mod 4) from nibble tables
+// (compact; see stage_skew_tables), t = 3 * (s >> 2) + (s & 3).  Position t
+// is the 256-byte block t >> 1 at half (t & 1) * 128, with nibble table q at
+// 32-byte position (q + group) & 3 of that half (group: s >> 2 for a
+// contiguous transform), so the four groups a warp covers in a distance-1
 // layer hit different banks.  A lookup address is one PRMT of a prepared
 // index byte into the block base.
 struct F16S : F16 {
-    uint32_t tab;   // shared-space address of slot 0 (256-byte aligned)
-    uint32_t ctab;  // shared-space address of the per-slot index-byte constants (16 B per slot)
+    uint32_t tab;   // shared-space address of position 0 (256-byte aligned)
+    uint32_t ctab;  // shared-space address of the per-position index bytes (4 B each)
     int lo;         // fftSkew index of slot 0
     using C = uint32_t;
     __device__ __forceinline__ C coef(int idx) const { return (uint32_t)(idx - lo); }
@@ -279,21 +287,23 @@ struct F16S : F16 {
         asm("ld.shared.u16 %0, [%1];" : "=r"(v) : "r"(addr));
         return v;
     }
-    // The position byte of nibble table q of slot s, replicated four times,
-    // is precomputed at staging (slot_consts) and read with one LDS.128.
-    // sw: the slot's bank swizzle (its butterfly group), chosen by the stager
-    static __device__ __forceinline__ uint32_t slot_const(uint32_t s, uint32_t q, uint32_t sw) {
-        return (((s & 1u) << 7) | (((q + sw) & 3u) << 5)) * 0x01010101u;
+    // Byte q of the position constant: the low address byte of nibble table q
+    // of position t (sw: the slot's bank swizzle, its butterfly group).
+    static __device__ __forceinline__ uint32_t pos_const(uint32_t t, uint32_t sw) {
+        uint32_t c = 0;
+#pragma unroll
+        for (uint32_t q = 0; q < 4; q++) c |= (((t & 1u) << 7) | (((q + sw) & 3u) << 5)) << (8 * q);
+        return c;
     }
-    __device__ __forceinline__ void mac(Q &x, Q y, C s) const {
-        const uint32_t base = tab + ((s >> 1) << 8);
-        uint32_t o0, o1, o2, o3;
-        asm("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
-                     : "=r"(o0), "=r"(o1), "=r"(o2), "=r"(o3) : "r"(ctab + (s << 4)));
-        const uint32_t n0 = ((y.x << 1) & 0x1E1E1E1Eu) | o0;  // 2 * symbol bits 0-3
-        const uint32_t n1 = ((y.x >> 3) & 0x1E1E1E1Eu) | o1;  // bits 4-7
-        const uint32_t n2 = ((y.y << 1) & 0x1E1E1E1Eu) | o2;  // bits 8-11
-        const uint32_t n3 = ((y.y >> 3) & 0x1E1E1E1Eu) | o3;  // bits 12-15
+    __device__ __forceinline__ void mac(Q &x, Q y, C t) const {
+        const uint32_t base = tab + ((t >> 1) << 8);
+        uint32_t k;
+        asm("ld.shared.u32 %0, [%1];" : "=r"(k) : "r"(ctab + (t << 2)));
+        // 2 * symbol bits 0-3, 4-7, 8-11, 12-15 with table q's byte in every lane
+        const uint32_t n0 = ((y.x << 1) & 0x1E1E1E1Eu) | __byte_perm(k, 0, 0x0000);
+        const uint32_t n1 = ((y.x >> 3) & 0x1E1E1E1Eu) | __byte_perm(k, 0, 0x1111);
+        const uint32_t n2 = ((y.y << 1) & 0x1E1E1E1Eu) | __byte_perm(k, 0, 0x2222);
+        const uint32_t n3 = ((y.y >> 3) & 0x1E1E1E1Eu) | __byte_perm(k, 0, 0x3333);
         uint32_t r[4];
 #pragma unroll
         for (int i = 0; i < 4; i++) {
@@ -307,31 +317,122 @@ struct F16S : F16 {
     }
 };
 
-// Copies the nibble tables of fftSkew indices [lo, lo + count) from the
-// skew-ordered global table ([65535][4][16] u16) into the F16S layout, and
-// writes each slot's index-byte constants to ctab.
-// index_of(s): the fftSkew index staged in slot s; swizzle_of(s): its bank
-// swizzle, which must differ between the (up to four) butterfly groups one
-// warp covers in a layer with distance 1.
-template <class IndexOf, class SwizzleOf>
-__device__ void stage_slots(uint8_t *tab, uint4 *ctab, const uint16_t *ts16, unsigned count, IndexOf index_of,
-                            SwizzleOf swizzle_of) {
-    for (unsigned v = threadIdx.x; v < count * 8; v += blockDim.x) {
-        const unsigned s = v >> 3, q = (v >> 1) & 3, h = v & 1;
-        const uint4 x = __ldg(reinterpret_cast<const uint4 *>(ts16 + (size_t)index_of(s) * 64 + q * 16) + h);
-        *reinterpret_cast<uint4 *>(tab + (s >> 1) * 256 + (s & 1) * 128 + ((q + swizzle_of(s)) & 3) * 32 + h * 16) = x;
+// F16S over compact positions: slots = 3 (mod 4) are left out.
+struct F16SC : F16S {
+    __device__ __forceinline__ C coef(int idx) const {
+        const uint32_t s = (uint32_t)(idx - lo);
+        return 3 * (s >> 2) + (s & 3);
     }
-    for (unsigned s = threadIdx.x; s < count; s += blockDim.x) {
-        const unsigned sw = swizzle_of(s);
-        ctab[s] = make_uint4(F16S::slot_const(s, 0, sw), F16S::slot_const(s, 1, sw), F16S::slot_const(s, 2, sw),
-                             F16S::slot_const(s, 3, sw));
+};
+
+// GF(2^16) products for butterfly layers of distance >= 4.  There the four
+// butterfly positions a warp covers belong to one group and share its
+// multiplier, so a warp's lookups all hit one table and a 64-entry table
+// costs no bank conflicts: a product takes three lookups instead of four.
+// Wide slot j (256 bytes, 256-byte aligned) holds, for one multiplier,
+// mulLog(e, lm) for e < 64 at bytes [0, 128) (symbol bits 0-5),
+// mulLog(e << 6, lm) for e < 32 at [128, 192) (bits 6-10) and
+// mulLog(e << 11, lm) for e < 32 at [192, 256) (bits 11-15); all zero when
+// lm is the modulus.  Those layers only use fftSkew indices = 3 (mod 4) (the
+// distance is a multiple of 4 and group starts are multiples of 4 * dist),
+// so the global source holds 16384 such tables, one per index 4j + 3.
+struct F16W : F16 {
+    uint32_t wtab;  // shared-space address of wide slot 0 (256-byte aligned)
+    int lo;         // fftSkew index that maps to slot position 0 (see coef)
+    using C = uint32_t;
+    // Wide slot of fftSkew index idx: (idx - lo) >> 2, for idx - lo = 3 (mod 4).
+    __device__ __forceinline__ C coef(int idx) const { return (uint32_t)(idx - lo) >> 2; }
+    __device__ __forceinline__ void mac(Q &x, Q y, C j) const {
+        const uint32_t base = wtab + (j << 8);
+        const uint32_t a0 = (y.x << 1) & 0x7E7E7E7Eu;                                            // 2 * bits 0-5
+        const uint32_t a1 = ((y.x >> 5) & 0x06060606u) | ((y.y << 3) & 0x38383838u) | 0x80808080u; // 128 + 2 * bits 6-10
+        const uint32_t a2 = ((y.y >> 2) & 0x3E3E3E3Eu) | 0xC0C0C0C0u;                            // 192 + 2 * bits 11-15
+        uint32_t r[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const uint32_t sel = 0x7650u | (uint32_t)i;
+            r[i] = F16S::lds16(__byte_perm(a0, base, sel)) ^ F16S::lds16(__byte_perm(a1, base, sel)) ^
+                   F16S::lds16(__byte_perm(a2, base, sel));
+        }
+        const uint32_t r01 = __byte_perm(r[0], r[1], 0x5410), r23 = __byte_perm(r[2], r[3], 0x5410);
+        x.x ^= __byte_perm(r01, r23, 0x6420);
+        x.y ^= __byte_perm(r01, r23, 0x7531);
+    }
+};
+
+// The field view a butterfly pass of distance >= 4 uses: the wide tables for
+// the staged GF(2^16) transforms, the same field otherwise.
+template <class F>
+struct WideOf {
+    using T = F;
+    static __device__ __forceinline__ const F &get(const F &f, uint32_t) { return f; }
+};
+template <class FS>
+struct WideOfStaged {
+    using T = F16W;
+    static __device__ __forceinline__ F16W get(const FS &f, uint32_t wtab) {
+        F16W v;
+        v.t = f.t;
+        v.skew = f.skew;
+        v.wtab = wtab;
+        v.lo = f.lo;
+        return v;
+    }
+};
+template <>
+struct WideOf<F16S> : WideOfStaged<F16S> {};
+template <>
+struct WideOf<F16SC> : WideOfStaged<F16SC> {};
+
+// Copies the wide tables of `count` slots: slot j gets the table of fftSkew
+// index index_of(j) (= 3 mod 4) from the global [16384][128] u16 source.
+template <class IndexOf>
+__device__ void stage_wide(uint8_t *wtab, const uint16_t *tw16, unsigned count, IndexOf index_of) {
+    for (unsigned v = threadIdx.x; v < count * 16; v += blockDim.x) {
+        const unsigned j = v >> 4, part = v & 15;
+        reinterpret_cast<uint4 *>(wtab + (size_t)j * 256)[part] =
+            __ldg(reinterpret_cast<const uint4 *>(tw16 + (size_t)(index_of(j) >> 2) * 128) + part);
     }
 }
 
+// Copies nibble tables from the skew-ordered global table ([65535][4][16]
+// u16) into positions [0, count) of the F16S layout, and writes each
+// position's index bytes to ctab.  index_of(t): the fftSkew index staged at
+// position t; swizzle_of(t): its bank swizzle, which must differ between the
+// (up to four) butterfly groups one warp covers in a layer with distance 1.
+template <class IndexOf, class SwizzleOf>
+__device__ void stage_slots(uint8_t *tab, uint32_t *ctab, const uint16_t *ts16, unsigned count, IndexOf index_of,
+                            SwizzleOf swizzle_of) {
+    for (unsigned v = threadIdx.x; v < count * 8; v += blockDim.x) {
+        const unsigned t = v >> 3, q = (v >> 1) & 3, h = v & 1;
+        const uint4 x = __ldg(reinterpret_cast<const uint4 *>(ts16 + (size_t)index_of(t) * 64 + q * 16) + h);
+        *reinterpret_cast<uint4 *>(tab + (t >> 1) * 256 + (t & 1) * 128 + ((q + swizzle_of(t)) & 3) * 32 + h * 16) = x;
+    }
+    for (unsigned t = threadIdx.x; t < count; t += blockDim.x) ctab[t] = F16S::pos_const(t, swizzle_of(t));
+}
+
+// Nibble positions of a contiguous transform of count slots: all of them, or
+// (compact) those of slots s != 3 (mod 4).
+__device__ __forceinline__ unsigned nibble_positions(unsigned count, bool compact) {
+    return compact ? count - count / 4 : count;
+}
+
 // Contiguous fftSkew indices: slot s = index - lo; group of slot s is s >> 2.
-__device__ void stage_skew_tables(uint8_t *tab, uint4 *ctab, const uint16_t *ts16, int lo, int count) {
-    stage_slots(tab, ctab, ts16, (unsigned)count, [lo](unsigned s) { return (unsigned)lo + s; },
-                [](unsigned s) { return s >> 2; });
+// With wide tables (wtab != nullptr, lo a multiple of 4) the slots s = 3
+// (mod 4) also go to wide slot s >> 2 for the layers of distance >= 4.  The
+// only other readers of those slots are distance-2 passes (an FFT over
+// 2^odd rows: slots r+1, r+3, r+5 of groups r = 0 mod 8); a transform
+// without one stages them only as wide tables (compact positions, F16S).
+__device__ void stage_skew_tables(uint8_t *tab, uint32_t *ctab, const uint16_t *ts16, int lo, int count,
+                                  bool compact, uint8_t *wtab = nullptr, const uint16_t *tw16 = nullptr) {
+    const unsigned npos = nibble_positions((unsigned)count, compact);
+    if (compact)
+        stage_slots(tab, ctab, ts16, npos, [lo](unsigned t) { return (unsigned)lo + 4 * (t / 3) + t % 3; },
+                    [](unsigned t) { return t / 3; });
+    else
+        stage_slots(tab, ctab, ts16, npos, [lo](unsigned s) { return (unsigned)lo + s; },
+                    [](unsigned s) { return s >> 2; });
+    if (wtab) stage_wide(wtab, tw16, (unsigned)count / 4, [lo](unsigned j) { return (unsigned)lo + 4 * j + 3; });
 }
 
 // Butterflies (galois_noasm.go:94-112; a log multiplier equal to the modulus
@@ -347,82 +448,108 @@ __device__ __forceinline__ void ifft2(const F &f, typename F::Q &x, typename F::
     f.mac(x, y, c);
 }
 
-// IFFT with decimation in time (ifftDITEncoder leopard.go:764-873 with
-// skew_off = m-1+block*m, ifftDITDecoder :650-693 with skew_off = -1): the
-// layer multipliers are skew[skew_off + iend], [+dist], [+2*dist].
+// One radix-4 pass of the IFFT with decimation in time (ifftDITEncoder
+// leopard.go:764-873 with skew_off = m-1+block*m, ifftDITDecoder :650-693
+// with skew_off = -1): layers dist and 2*dist, multipliers
+// skew[skew_off + iend], [+dist], [+2*dist]; groups start below mtrunc.
 template <class F>
-__device__ void ifft_rows(const F &f, uint8_t *w, unsigned mtrunc, unsigned m, int skew_off) {
+__device__ void ifft_pass4(const F &f, uint8_t *w, unsigned mtrunc, unsigned dist, unsigned ld, int skew_off) {
     using Q = typename F::Q;
+    const unsigned groups = (mtrunc + (dist << 2) - 1) >> (ld + 2);
+    const unsigned items = (groups << ld) << F::kQuadShift;
+    for (unsigned it = threadIdx.x; it < items; it += blockDim.x) {
+        const unsigned q = it >> F::kQuadShift, c = it & (F::kQuads - 1);
+        const unsigned r = (q >> ld) << (ld + 2), i = r + (q & (dist - 1)), iend = r + dist;
+        const typename F::C m01 = f.coef(skew_off + (int)iend);
+        const typename F::C m02 = f.coef(skew_off + (int)(iend + dist));
+        const typename F::C m23 = f.coef(skew_off + (int)(iend + 2 * dist));
+        uint8_t *p0 = w + (size_t)i * kLeoTile;
+        uint8_t *p1 = p0 + (size_t)dist * kLeoTile, *p2 = p1 + (size_t)dist * kLeoTile,
+                *p3 = p2 + (size_t)dist * kLeoTile;
+        Q x0 = F::ld(p0, c), x1 = F::ld(p1, c), x2 = F::ld(p2, c), x3 = F::ld(p3, c);
+        ifft2(f, x0, x1, m01);
+        ifft2(f, x2, x3, m23);
+        ifft2(f, x0, x2, m02);
+        ifft2(f, x1, x3, m02);
+        F::st(p0, c, x0);
+        F::st(p1, c, x1);
+        F::st(p2, c, x2);
+        F::st(p3, c, x3);
+    }
+    __syncthreads();
+}
+
+// The radix-2 IFFT layer left when log2(m) is odd (dist == m / 2).
+template <class F>
+__device__ void ifft_pass2(const F &f, uint8_t *w, unsigned dist, int skew_off) {
+    using Q = typename F::Q;
+    const typename F::C lm = f.coef(skew_off + (int)dist);
+    const unsigned items = dist << F::kQuadShift;
+    for (unsigned it = threadIdx.x; it < items; it += blockDim.x) {
+        const unsigned i = it >> F::kQuadShift, c = it & (F::kQuads - 1);
+        uint8_t *p0 = w + (size_t)i * kLeoTile, *p1 = p0 + (size_t)dist * kLeoTile;
+        Q x = F::ld(p0, c), y = F::ld(p1, c);
+        ifft2(f, x, y, lm);
+        F::st(p0, c, x);
+        F::st(p1, c, y);
+    }
+    __syncthreads();
+}
+
+// IFFT over m rows.  Passes of distance >= 4 use the field's wide view
+// (WideOf; wtab: shared address of the wide slots, staged GF(2^16) only).
+template <class F>
+__device__ void ifft_rows(const F &f, uint8_t *w, unsigned mtrunc, unsigned m, int skew_off, uint32_t wtab = 0) {
     unsigned dist = 1, dist4 = 4, ld = 0;  // dist == 1 << ld
     for (; dist4 <= m; dist = dist4, dist4 <<= 2, ld += 2) {
-        const unsigned groups = (mtrunc + dist4 - 1) >> (ld + 2);
-        const unsigned items = (groups << ld) << F::kQuadShift;
-        for (unsigned it = threadIdx.x; it < items; it += blockDim.x) {
-            const unsigned q = it >> F::kQuadShift, c = it & (F::kQuads - 1);
-            const unsigned r = (q >> ld) << (ld + 2), i = r + (q & (dist - 1)), iend = r + dist;
-            const typename F::C m01 = f.coef(skew_off + (int)iend);
-            const typename F::C m02 = f.coef(skew_off + (int)(iend + dist));
-            const typename F::C m23 = f.coef(skew_off + (int)(iend + 2 * dist));
-            uint8_t *p0 = w + (size_t)i * kLeoTile;
-            uint8_t *p1 = p0 + (size_t)dist * kLeoTile, *p2 = p1 + (size_t)dist * kLeoTile,
-                    *p3 = p2 + (size_t)dist * kLeoTile;
-            Q x0 = F::ld(p0, c), x1 = F::ld(p1, c), x2 = F::ld(p2, c), x3 = F::ld(p3, c);
-            ifft2(f, x0, x1, m01);
-            ifft2(f, x2, x3, m23);
-            ifft2(f, x0, x2, m02);
-            ifft2(f, x1, x3, m02);
-            F::st(p0, c, x0);
-            F::st(p1, c, x1);
-            F::st(p2, c, x2);
-            F::st(p3, c, x3);
-        }
-        __syncthreads();
+        if (dist >= 4) ifft_pass4(WideOf<F>::get(f, wtab), w, mtrunc, dist, ld, skew_off);
+        else ifft_pass4(f, w, mtrunc, dist, ld, skew_off);
     }
     if (dist < m) {  // one radix-2 layer left (dist == m / 2)
-        const typename F::C lm = f.coef(skew_off + (int)dist);
-        const unsigned items = dist << F::kQuadShift;
-        for (unsigned it = threadIdx.x; it < items; it += blockDim.x) {
-            const unsigned i = it >> F::kQuadShift, c = it & (F::kQuads - 1);
-            uint8_t *p0 = w + (size_t)i * kLeoTile, *p1 = p0 + (size_t)dist * kLeoTile;
-            Q x = F::ld(p0, c), y = F::ld(p1, c);
-            ifft2(f, x, y, lm);
-            F::st(p0, c, x);
-            F::st(p1, c, y);
-        }
-        __syncthreads();
+        if (dist >= 4) ifft_pass2(WideOf<F>::get(f, wtab), w, dist, skew_off);
+        else ifft_pass2(f, w, dist, skew_off);
     }
 }
 
-// FFT with decimation in time (fftDIT leopard.go:696-736): multipliers
-// skew[iend-1], [iend+dist-1], [iend+2*dist-1]; groups start below mtrunc.
+// One radix-4 pass of the FFT with decimation in time (fftDIT
+// leopard.go:696-736): multipliers skew[iend-1], [iend+dist-1],
+// [iend+2*dist-1]; groups start below mtrunc.
 template <class F>
-__device__ void fft_rows(const F &f, uint8_t *w, unsigned mtrunc, unsigned m) {
+__device__ void fft_pass4(const F &f, uint8_t *w, unsigned mtrunc, unsigned dist, unsigned ld) {
+    using Q = typename F::Q;
+    const unsigned groups = (mtrunc + (dist << 2) - 1) >> (ld + 2);
+    const unsigned items = (groups << ld) << F::kQuadShift;
+    for (unsigned it = threadIdx.x; it < items; it += blockDim.x) {
+        const unsigned q = it >> F::kQuadShift, c = it & (F::kQuads - 1);
+        const unsigned r = (q >> ld) << (ld + 2), i = r + (q & (dist - 1)), iend = r + dist;
+        const typename F::C m01 = f.coef((int)iend - 1), m02 = f.coef((int)(iend + dist) - 1),
+                            m23 = f.coef((int)(iend + 2 * dist) - 1);
+        uint8_t *p0 = w + (size_t)i * kLeoTile;
+        uint8_t *p1 = p0 + (size_t)dist * kLeoTile, *p2 = p1 + (size_t)dist * kLeoTile,
+                *p3 = p2 + (size_t)dist * kLeoTile;
+        Q x0 = F::ld(p0, c), x1 = F::ld(p1, c), x2 = F::ld(p2, c), x3 = F::ld(p3, c);
+        fft2(f, x0, x2, m02);
+        fft2(f, x1, x3, m02);
+        fft2(f, x0, x1, m01);
+        fft2(f, x2, x3, m23);
+        F::st(p0, c, x0);
+        F::st(p1, c, x1);
+        F::st(p2, c, x2);
+        F::st(p3, c, x3);
+    }
+    __syncthreads();
+}
+
+// FFT over m rows; passes of distance >= 4 use the wide view (see ifft_rows).
+template <class F>
+__device__ void fft_rows(const F &f, uint8_t *w, unsigned mtrunc, unsigned m, uint32_t wtab = 0) {
     using Q = typename F::Q;
     unsigned dist4 = m, dist = m >> 2;
     unsigned ld = 0;  // dist == 1 << ld
     while ((2u << ld) <= dist) ld++;
     for (; dist != 0; dist4 = dist, dist >>= 2, ld -= 2) {
-        const unsigned groups = (mtrunc + dist4 - 1) >> (ld + 2);
-        const unsigned items = (groups << ld) << F::kQuadShift;
-        for (unsigned it = threadIdx.x; it < items; it += blockDim.x) {
-            const unsigned q = it >> F::kQuadShift, c = it & (F::kQuads - 1);
-            const unsigned r = (q >> ld) << (ld + 2), i = r + (q & (dist - 1)), iend = r + dist;
-            const typename F::C m01 = f.coef((int)iend - 1), m02 = f.coef((int)(iend + dist) - 1),
-                                m23 = f.coef((int)(iend + 2 * dist) - 1);
-            uint8_t *p0 = w + (size_t)i * kLeoTile;
-            uint8_t *p1 = p0 + (size_t)dist * kLeoTile, *p2 = p1 + (size_t)dist * kLeoTile,
-                    *p3 = p2 + (size_t)dist * kLeoTile;
-            Q x0 = F::ld(p0, c), x1 = F::ld(p1, c), x2 = F::ld(p2, c), x3 = F::ld(p3, c);
-            fft2(f, x0, x2, m02);
-            fft2(f, x1, x3, m02);
-            fft2(f, x0, x1, m01);
-            fft2(f, x2, x3, m23);
-            F::st(p0, c, x0);
-            F::st(p1, c, x1);
-            F::st(p2, c, x2);
-            F::st(p3, c, x3);
-        }
-        __syncthreads();
+        if (dist >= 4) fft_pass4(WideOf<F>::get(f, wtab), w, mtrunc, dist, ld);
+        else fft_pass4(f, w, mtrunc, dist, ld);
     }
     if (dist4 == 2) {
         const unsigned items = ((mtrunc + 1) / 2) << F::kQuadShift;
@@ -525,16 +652,51 @@ __global__ void __launch_bounds__(kLeoThreads) leo_encode_kernel(const __grid_co
     }
 }
 
+// Shared layout of the staged GF(2^16) encode for m rows per block: 2m data
+// rows, the nibble positions (256-byte blocks of two), the wide slots of the
+// indices = 3 (mod 4), the 4-byte position constants.  The IFFTs never read
+// slots = 3 (mod 4) from nibble tables, nor does an FFT over 2^even rows;
+// an FFT over 2^odd rows has a distance-2 pass that does, so m = 2^odd keeps
+// every nibble position.
+struct EncLayout {
+    unsigned rows_bytes, nib_pos, wide, tab_bytes, wide_bytes;
+    __host__ __device__ explicit EncLayout(unsigned m) {
+        const unsigned count = m - 1;
+        const bool odd = log2u(m) & 1;
+        rows_bytes = 2 * m * kLeoTile;
+        nib_pos = odd ? count : count - count / 4;
+        wide = count / 4;
+        tab_bytes = (nib_pos + 1) / 2 * 256;
+        wide_bytes = wide * 256;
+    }
+    __host__ __device__ static unsigned log2u(unsigned v) {  // v a power of two
+        unsigned n = 0;
+        while (v > 1) {
+            v >>= 1;
+            n++;
+        }
+        return n;
+    }
+    __host__ __device__ size_t bytes() const { return (size_t)rows_bytes + tab_bytes + wide_bytes + nib_pos * 4 + 256; }
+};
+
 // GF(2^16) encode with each transform's multiplier tables staged in shared
-// memory (F16S): 2m data rows plus (m-1) 128-byte table slots, used while
-// that fits one CTA (m <= 512).
-__global__ void __launch_bounds__(kLeoThreads) leo_encode16_staged_kernel(const __grid_constant__ LeoEncArgs a) {
+// memory (F16S nibble positions for the distance-1 and -2 passes, F16W wide
+// slots for the passes of distance >= 4; EncLayout), used while that fits one
+// CTA (m <= 512).  Block size: 2m threads up to 512, one butterfly quad per
+// thread in a radix-4 pass; at m = 256, 74.5 KB and 40 registers, so three
+// CTAs per SM.
+__global__ void __launch_bounds__(kLeoEncThreadsMax) leo_encode16_staged_kernel(const __grid_constant__ LeoEncArgs a) {
     extern __shared__ __align__(16) uint8_t sm[];
     const unsigned m = (unsigned)a.m;
+    const EncLayout L(m);
     uint8_t *acc = sm, *tmp = sm + (size_t)m * kLeoTile;
     uint8_t *tab = align_shared256(tmp + (size_t)m * kLeoTile);
-    uint4 *ctab = reinterpret_cast<uint4 *>(tab + (size_t)(m / 2) * 256);
-    F16S f;
+    uint8_t *wtab = tab + L.tab_bytes;
+    uint32_t *ctab = reinterpret_cast<uint32_t *>(wtab + L.wide_bytes);
+    const uint32_t wtab_s = (uint32_t)__cvta_generic_to_shared(wtab);
+    const bool fft_compact = L.nib_pos != m - 1;
+    F16SC f;  // the IFFTs use compact positions
     f.t = a.t16;
     f.skew = a.skew;
     f.tab = (uint32_t)__cvta_generic_to_shared(tab);
@@ -543,17 +705,17 @@ __global__ void __launch_bounds__(kLeoThreads) leo_encode16_staged_kernel(const 
     const int cnt0 = a.k < (int)m ? a.k : (int)m;
     load_rows<F16>(acc, a.shard, 0, cnt0, (int)m, off);
     f.lo = (int)m;  // block 0 reads fftSkew[m .. 2m-2]
-    stage_skew_tables(tab, ctab, a.ts16, f.lo, (int)m - 1);
+    stage_skew_tables(tab, ctab, a.ts16, f.lo, (int)m - 1, true, wtab, a.tw16);
     __syncthreads();
-    ifft_rows(f, acc, (unsigned)cnt0, m, (int)m - 1);
+    ifft_rows(f, acc, (unsigned)cnt0, m, (int)m - 1, wtab_s);
     for (int b = 1; b * (int)m < a.k; b++) {
         const int start = b * (int)m;
         const int cnt = a.k - start < (int)m ? a.k - start : (int)m;
         load_rows<F16>(tmp, a.shard, start, cnt, (int)m, off);
         f.lo = (int)m + b * (int)m;
-        stage_skew_tables(tab, ctab, a.ts16, f.lo, (int)m - 1);
+        stage_skew_tables(tab, ctab, a.ts16, f.lo, (int)m - 1, true, wtab, a.tw16);
         __syncthreads();
-        ifft_rows(f, tmp, (unsigned)cnt, m, (int)m - 1 + b * (int)m);
+        ifft_rows(f, tmp, (unsigned)cnt, m, (int)m - 1 + b * (int)m, wtab_s);
         for (int v = threadIdx.x; v < (int)m * 4; v += blockDim.x) {
             uint4 x = reinterpret_cast<uint4 *>(acc)[v];
             const uint4 y = reinterpret_cast<const uint4 *>(tmp)[v];
@@ -566,9 +728,10 @@ __global__ void __launch_bounds__(kLeoThreads) leo_encode16_staged_kernel(const 
         __syncthreads();
     }
     f.lo = 0;  // the FFT reads fftSkew[0 .. m-2]
-    stage_skew_tables(tab, ctab, a.ts16, 0, (int)m - 1);
+    stage_skew_tables(tab, ctab, a.ts16, 0, (int)m - 1, fft_compact, wtab, a.tw16);
     __syncthreads();
-    fft_rows(f, acc, (unsigned)a.p, m);
+    if (fft_compact) fft_rows(f, acc, (unsigned)a.p, m, wtab_s);
+    else fft_rows(static_cast<const F16S &>(f), acc, (unsigned)a.p, m, wtab_s);
     for (int v = threadIdx.x; v < a.p * F16::kRowParts; v += blockDim.x) {
         const int r = v / F16::kRowParts, c = v % F16::kRowParts;
         F16::row_out(const_cast<uint8_t *>(a.shard[a.k + r]) + off, acc + (size_t)r * kLeoTile, c);
@@ -584,76 +747,112 @@ __global__ void __launch_bounds__(kLeoThreads) leo_encode16_staged_kernel(const 
 __device__ void formal_derivative(uint8_t *w, unsigned n);
 
 constexpr unsigned kDecChunkSlots = 672;
-constexpr size_t kDecTableBytes = (size_t)kDecChunkSlots / 2 * 256 + (size_t)kDecChunkSlots * 16;
+constexpr size_t kDecTableBytes = 98304;  // >= kDecChunkSlots / 2 * 256 + kDecChunkSlots * 4
+constexpr unsigned kDecWideSlots = kDecTableBytes / 256;  // 128 groups of 3 wide slots
+static_assert((size_t)kDecChunkSlots / 2 * 256 + (size_t)kDecChunkSlots * 4 <= kDecTableBytes, "nibble chunk");
 
-template <bool kFft>
-__device__ void radix4_staged(const F16S &f, uint8_t *w, uint8_t *tab, uint4 *ctab, const uint16_t *ts16,
-                              unsigned mtrunc, unsigned dist, unsigned ld) {
+// The butterflies of groups g0 .. g0+cnt-1 of one radix-4 pass whose
+// multipliers sit in slots 3*(g - g0) + (0: m01, 1: m02, 2: m23) of the
+// field view f (nibble slots for distances 1 and 2, wide ones from 4).
+template <bool kFft, class FV>
+__device__ void radix4_chunk(const FV &f, uint8_t *w, unsigned g0, unsigned cnt, unsigned dist, unsigned ld) {
     using Q = F16::Q;
+    const unsigned items = (cnt << ld) << F16::kQuadShift;
+    for (unsigned it = threadIdx.x; it < items; it += blockDim.x) {
+        const unsigned q = it >> F16::kQuadShift, c = it & (F16::kQuads - 1);
+        const unsigned gl = q >> ld;
+        const unsigned r = (g0 + gl) << (ld + 2), i = r + (q & (dist - 1));
+        const uint32_t s01 = gl * 3, s02 = s01 + 1, s23 = s01 + 2;
+        uint8_t *p0 = w + (size_t)i * kLeoTile;
+        uint8_t *p1 = p0 + (size_t)dist * kLeoTile, *p2 = p1 + (size_t)dist * kLeoTile,
+                *p3 = p2 + (size_t)dist * kLeoTile;
+        Q x0 = F16::ld(p0, c), x1 = F16::ld(p1, c), x2 = F16::ld(p2, c), x3 = F16::ld(p3, c);
+        if (kFft) {
+            fft2(f, x0, x2, s02);
+            fft2(f, x1, x3, s02);
+            fft2(f, x0, x1, s01);
+            fft2(f, x2, x3, s23);
+        } else {
+            ifft2(f, x0, x1, s01);
+            ifft2(f, x2, x3, s23);
+            ifft2(f, x0, x2, s02);
+            ifft2(f, x1, x3, s02);
+        }
+        F16::st(p0, c, x0);
+        F16::st(p1, c, x1);
+        F16::st(p2, c, x2);
+        F16::st(p3, c, x3);
+    }
+    __syncthreads();
+}
+
+// Slot t of group g holds fftSkew[4*dist*g + (t+1)*dist - 1].  From distance
+// 4 on those indices are = 3 (mod 4) and the wide tables are staged instead,
+// up to 128 groups per chunk.
+template <bool kFft>
+__device__ void radix4_staged(const F16S &f, uint8_t *w, uint8_t *tab, uint32_t *ctab, const uint16_t *ts16,
+                              const uint16_t *tw16, unsigned mtrunc, unsigned dist, unsigned ld) {
     const unsigned groups = (mtrunc + (dist << 2) - 1) >> (ld + 2);
+    const auto index_of = [=](unsigned g0) {
+        return [=](unsigned s) { return 4 * dist * (g0 + s / 3) + (s % 3 + 1) * dist - 1; };
+    };
+    if (dist >= 4) {
+        const F16W fw = WideOf<F16S>::get(f, (uint32_t)__cvta_generic_to_shared(tab));
+        constexpr unsigned kPer = kDecWideSlots / 3;
+        for (unsigned g0 = 0; g0 < groups; g0 += kPer) {
+            const unsigned cnt = groups - g0 < kPer ? groups - g0 : kPer;
+            stage_wide(tab, tw16, cnt * 3, index_of(g0));
+            __syncthreads();
+            radix4_chunk<kFft>(fw, w, g0, cnt, dist, ld);
+        }
+        return;
+    }
     constexpr unsigned kPer = kDecChunkSlots / 3;
     for (unsigned g0 = 0; g0 < groups; g0 += kPer) {
         const unsigned cnt = groups - g0 < kPer ? groups - g0 : kPer;
-        stage_slots(tab, ctab, ts16, cnt * 3,
-                    [=](unsigned s) { return 4 * dist * (g0 + s / 3) + (s % 3 + 1) * dist - 1; },
-                    [](unsigned s) { return s / 3; });
+        stage_slots(tab, ctab, ts16, cnt * 3, index_of(g0), [](unsigned s) { return s / 3; });
         __syncthreads();
-        const unsigned items = (cnt << ld) << F16::kQuadShift;
-        for (unsigned it = threadIdx.x; it < items; it += blockDim.x) {
-            const unsigned q = it >> F16::kQuadShift, c = it & (F16::kQuads - 1);
-            const unsigned gl = q >> ld;
-            const unsigned r = (g0 + gl) << (ld + 2), i = r + (q & (dist - 1));
-            const uint32_t s01 = gl * 3, s02 = s01 + 1, s23 = s01 + 2;
-            uint8_t *p0 = w + (size_t)i * kLeoTile;
-            uint8_t *p1 = p0 + (size_t)dist * kLeoTile, *p2 = p1 + (size_t)dist * kLeoTile,
-                    *p3 = p2 + (size_t)dist * kLeoTile;
-            Q x0 = F16::ld(p0, c), x1 = F16::ld(p1, c), x2 = F16::ld(p2, c), x3 = F16::ld(p3, c);
-            if (kFft) {
-                fft2(f, x0, x2, s02);
-                fft2(f, x1, x3, s02);
-                fft2(f, x0, x1, s01);
-                fft2(f, x2, x3, s23);
-            } else {
-                ifft2(f, x0, x1, s01);
-                ifft2(f, x2, x3, s23);
-                ifft2(f, x0, x2, s02);
-                ifft2(f, x1, x3, s02);
-            }
-            F16::st(p0, c, x0);
-            F16::st(p1, c, x1);
-            F16::st(p2, c, x2);
-            F16::st(p3, c, x3);
-        }
-        __syncthreads();
+        radix4_chunk<kFft>(f, w, g0, cnt, dist, ld);
     }
 }
 
 // ifftDITDecoder (leopard.go:650-693) over n rows, groups below mtrunc.
-__device__ void ifft_staged(const F16S &f, uint8_t *w, uint8_t *tab, uint4 *ctab, const uint16_t *ts16,
-                            unsigned mtrunc, unsigned n) {
+__device__ void ifft_staged(const F16S &f, uint8_t *w, uint8_t *tab, uint32_t *ctab, const uint16_t *ts16,
+                            const uint16_t *tw16, unsigned mtrunc, unsigned n) {
     unsigned dist = 1, dist4 = 4, ld = 0;
-    for (; dist4 <= n; dist = dist4, dist4 <<= 2, ld += 2) radix4_staged<false>(f, w, tab, ctab, ts16, mtrunc, dist, ld);
+    for (; dist4 <= n; dist = dist4, dist4 <<= 2, ld += 2)
+        radix4_staged<false>(f, w, tab, ctab, ts16, tw16, mtrunc, dist, ld);
     if (dist < n) {  // one radix-2 layer left (dist == n / 2): multiplier fftSkew[dist - 1]
-        stage_slots(tab, ctab, ts16, 1, [=](unsigned) { return dist - 1; }, [](unsigned) { return 0u; });
-        __syncthreads();
-        for (unsigned it = threadIdx.x; it < (dist << F16::kQuadShift); it += blockDim.x) {
-            const unsigned i = it >> F16::kQuadShift, c = it & (F16::kQuads - 1);
-            uint8_t *p0 = w + (size_t)i * kLeoTile, *p1 = p0 + (size_t)dist * kLeoTile;
-            F16::Q x = F16::ld(p0, c), y = F16::ld(p1, c);
-            ifft2(f, x, y, 0u);
-            F16::st(p0, c, x);
-            F16::st(p1, c, y);
+        auto layer = [&](const auto &fv) {
+            for (unsigned it = threadIdx.x; it < (dist << F16::kQuadShift); it += blockDim.x) {
+                const unsigned i = it >> F16::kQuadShift, c = it & (F16::kQuads - 1);
+                uint8_t *p0 = w + (size_t)i * kLeoTile, *p1 = p0 + (size_t)dist * kLeoTile;
+                F16::Q x = F16::ld(p0, c), y = F16::ld(p1, c);
+                ifft2(fv, x, y, 0u);
+                F16::st(p0, c, x);
+                F16::st(p1, c, y);
+            }
+            __syncthreads();
+        };
+        if (dist >= 4) {
+            stage_wide(tab, tw16, 1, [=](unsigned) { return dist - 1; });
+            __syncthreads();
+            layer(WideOf<F16S>::get(f, (uint32_t)__cvta_generic_to_shared(tab)));
+        } else {
+            stage_slots(tab, ctab, ts16, 1, [=](unsigned) { return dist - 1; }, [](unsigned) { return 0u; });
+            __syncthreads();
+            layer(f);
         }
-        __syncthreads();
     }
 }
 
 // fftDIT (leopard.go:696-736) over n rows, groups below mtrunc.
-__device__ void fft_staged(const F16S &f, uint8_t *w, uint8_t *tab, uint4 *ctab, const uint16_t *ts16,
-                           unsigned mtrunc, unsigned n) {
+__device__ void fft_staged(const F16S &f, uint8_t *w, uint8_t *tab, uint32_t *ctab, const uint16_t *ts16,
+                           const uint16_t *tw16, unsigned mtrunc, unsigned n) {
     unsigned dist4 = n, dist = n >> 2, ld = 0;
     while ((2u << ld) <= dist) ld++;
-    for (; dist != 0; dist4 = dist, dist >>= 2, ld -= 2) radix4_staged<true>(f, w, tab, ctab, ts16, mtrunc, dist, ld);
+    for (; dist != 0; dist4 = dist, dist >>= 2, ld -= 2)
+        radix4_staged<true>(f, w, tab, ctab, ts16, tw16, mtrunc, dist, ld);
     if (dist4 == 2) {  // final radix-2 layer: pair (r, r+1) multiplied by fftSkew[r]
         const unsigned pairs = (mtrunc + 1) / 2;
         for (unsigned p0 = 0; p0 < pairs; p0 += kDecChunkSlots) {
@@ -678,7 +877,7 @@ __global__ void __launch_bounds__(kLeoDecodeThreads) leo_decode16_staged_kernel(
     const unsigned n = (unsigned)a.n, m = (unsigned)a.m;
     uint8_t *w = sm;
     uint8_t *tab = align_shared256(w + (size_t)n * kLeoTile);
-    uint4 *ctab = reinterpret_cast<uint4 *>(tab + (size_t)kDecChunkSlots / 2 * 256);
+    uint32_t *ctab = reinterpret_cast<uint32_t *>(tab + (size_t)kDecChunkSlots / 2 * 256);
     F16 fg;  // log-indexed tables for the per-row error-locator products
     fg.t = a.t16;
     fg.skew = a.skew;
@@ -699,9 +898,9 @@ __global__ void __launch_bounds__(kLeoDecodeThreads) leo_decode16_staged_kernel(
         F16::st(w + (size_t)r * kLeoTile, c, v);
     }
     __syncthreads();
-    ifft_staged(fs, w, tab, ctab, a.ts16, (unsigned)a.input_count, n);
+    ifft_staged(fs, w, tab, ctab, a.ts16, a.tw16, (unsigned)a.input_count, n);
     formal_derivative(w, n);
-    fft_staged(fs, w, tab, ctab, a.ts16, m + (unsigned)a.k, n);
+    fft_staged(fs, w, tab, ctab, a.ts16, a.tw16, m + (unsigned)a.k, n);
     const unsigned total = (unsigned)(a.k + a.p) << F16::kQuadShift;
     for (unsigned it = threadIdx.x; it < total; it += blockDim.x) {
         const int i = (int)(it >> F16::kQuadShift), c = (int)(it & (F16::kQuads - 1));
@@ -714,7 +913,7 @@ __global__ void __launch_bounds__(kLeoDecodeThreads) leo_decode16_staged_kernel(
 
 // Shared bytes of the staged GF(2^16) encode (0 when it does not fit a CTA).
 size_t staged_encode_smem(unsigned m) {
-    const size_t bytes = (size_t)2 * m * kLeoTile + (size_t)(m / 2) * 256 + (size_t)m * 16 + 256;
+    const size_t bytes = EncLayout(m).bytes();
     return bytes <= 227u * 1024u ? bytes : 0;
 }
 
@@ -1123,6 +1322,24 @@ __global__ void build_ts16(uint16_t *t, const uint16_t *skew, const uint16_t *lo
     }
 }
 
+// Builds the wide tables of F16W: row j serves fftSkew index 4j + 3 (zero
+// past the table or where the skew is the modulus); entries mulLog(e, lm)
+// (e < 64), mulLog(e << 6, lm) and mulLog(e << 11, lm) (e < 32).
+__global__ void build_tw16(uint16_t *t, const uint16_t *skew, const uint16_t *log, const uint16_t *exp) {
+    for (unsigned idx = blockIdx.x * blockDim.x + threadIdx.x; idx < 16384u * 128u; idx += gridDim.x * blockDim.x) {
+        const unsigned j = idx >> 7, e = idx & 127, i = 4 * j + 3;
+        const unsigned lm = i < 65535u ? skew[i] : 65535u;
+        const unsigned x = e < 64 ? e : (e < 96 ? (e - 64) << 6 : (e - 96) << 11);
+        uint16_t v = 0;
+        if (x && lm != 65535u) {
+            unsigned s = (unsigned)log[x] + lm;
+            s = (s + (s >> 16)) & 0xFFFF;
+            v = exp[s];
+        }
+        t[idx] = v;
+    }
+}
+
 int ensure_tables(rsgpu_encoder *enc) {
     rsgpu_ctx *ctx = enc->ctx;
     if (enc->leo && enc->leo->device == ctx->device) return RS_OK;
@@ -1161,6 +1378,9 @@ int ensure_tables(rsgpu_encoder *enc) {
     RS_CUDA(cudaGetLastError());
     RS_CUDA(cudaMalloc(&st->ts16, 65535ull * 64 * 2));
     build_ts16<<<1024, 256, 0, ctx->stream>>>(st->ts16, st->skew16, dlog, dexp);
+    RS_CUDA(cudaGetLastError());
+    RS_CUDA(cudaMalloc(&st->tw16, 16384ull * 128 * 2));
+    build_tw16<<<1024, 256, 0, ctx->stream>>>(st->tw16, st->skew16, dlog, dexp);
     RS_CUDA(cudaGetLastError());
     RS_CUDA(cudaStreamSynchronize(ctx->stream));
     cudaFree(dlog);
@@ -1391,6 +1611,7 @@ int leo_encode_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, size_t size, 
     a.skew = g16 ? enc->leo->skew16 : enc->leo->skew8;
     a.t16 = enc->leo->t16;
     a.ts16 = enc->leo->ts16;
+    a.tw16 = enc->leo->tw16;
     a.t8 = enc->leo->t8;
     const size_t smem = (size_t)2 * m * kLeoTile + (g16 ? 0 : kT8Bytes + kT8Slack);
     const int grid = (int)(size / kLeoTile);
@@ -1399,7 +1620,8 @@ int leo_encode_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, size_t size, 
     if (staged && m >= 4) {
         rc = set_smem(leo_encode16_staged_kernel, staged);
         if (rc) return rc;
-        leo_encode16_staged_kernel<<<grid, kLeoThreads, staged, st>>>(a);
+        const int threads = (int)std::min<unsigned>(kLeoEncThreadsMax, std::max(64u, 2 * m));
+        leo_encode16_staged_kernel<<<grid, threads, staged, st>>>(a);
     } else if (g16) {
         rc = set_smem(leo_encode_kernel<F16>, smem);
         if (rc) return rc;
@@ -1549,6 +1771,7 @@ int leo_reconstruct_enqueue(rsgpu_encoder *enc, uint8_t *const *shards, const ui
     a->skew = g16 ? enc->leo->skew16 : enc->leo->skew8;
     a->t16 = enc->leo->t16;
     a->ts16 = enc->leo->ts16;
+    a->tw16 = enc->leo->tw16;
     a->t8 = enc->leo->t8;
     const size_t smem = g16 ? (size_t)n * kLeoTile + kDecTableBytes + 256 : (size_t)n * kLeoTile + kT8Bytes + kT8Slack;
     const int grid = (int)(size / kLeoTile);
