@@ -521,6 +521,18 @@ def lookup_ceiling_gproducts(dev, lookups_per_product):
     return sms * mhz * 1e6 * 32 / lookups_per_product / 1e9
 
 
+def leo16_lookups_per_product(lg, iffts):
+    """Average shared-memory lookups per GF(2^16) product of `iffts` IFFTs and
+    one FFT over 2^lg rows (every layer has the same number of butterflies):
+    4 in the layers of the IFFT's distance-1 radix-4 pass, of the FFT's last
+    radix-4 pass and of its final radix-2 layer when lg is odd; 3 elsewhere."""
+    nib_i = min(lg, 2)
+    nib_f = min(lg, 3 if lg % 2 else 2)
+    layers = (iffts + 1) * lg
+    nib = iffts * nib_i + nib_f
+    return (4 * nib + 3 * (layers - nib)) / layers
+
+
 def extra_leopard(dev, cpu_seconds=2.0):
     """C4: Leopard GF(2^16) 1000+200 x 64 KiB and GF(2^8) 192+56 x 256 KiB
     encode / reconstruct (p random erasures), device-resident.  Rebuilt shards
@@ -582,9 +594,15 @@ def extra_leopard(dev, cpu_seconds=2.0):
         enc_products = ((k + m - 1) // m + 1) * (m // 2) * lg(m) * syms
         dec_products = 2 * (n // 2) * lg(n) * syms
         threads, ce, cr = leopard_cpu(gf, k, p, [s.cpu().numpy() for s in sh], lost, cpu_seconds)
-        # lookup ceiling: one shared-memory lookup per lane per clock per SM,
-        # 4 lookups per GF(2^16) product (nibble tables), 2 per GF(2^8)
-        ceiling = lookup_ceiling_gproducts(dev, 4 if gf == 16 else 2)
+        # lookup ceiling: one shared-memory lookup per lane per clock per SM;
+        # GF(2^8) products take 2 lookups; GF(2^16) ones 4 (nibble tables) in
+        # the passes of distance 1 and 2 and 3 (split tables) from distance 4
+        if gf == 16:
+            lk_e = leo16_lookups_per_product(lg(m), (k + m - 1) // m)
+            lk_d = leo16_lookups_per_product(lg(n), 1)
+        else:
+            lk_e = lk_d = 2.0
+        ceil_e, ceil_d = lookup_ceiling_gproducts(dev, lk_e), lookup_ceiling_gproducts(dev, lk_d)
         out[name] = {"encode_ms": round(ms_e, 4), "encode_data_GBps": round(k * size / (ms_e / 1e3) / 1e9, 1),
                      "encode_frac_of_hbm": round((k + p) * size / (ms_e / 1e3) / 1e9 / peaks()[0], 4),
                      "encode_Gproducts_per_s": round(enc_products / (ms_e / 1e3) / 1e9, 1),
@@ -592,11 +610,13 @@ def extra_leopard(dev, cpu_seconds=2.0):
                      "reconstruct_data_GBps": round(k * size / (ms_r / 1e3) / 1e9, 1),
                      "reconstruct_frac_of_hbm": round((k + p) * size / (ms_r / 1e3) / 1e9 / peaks()[0], 4),
                      "reconstruct_Gproducts_per_s": round(dec_products / (ms_r / 1e3) / 1e9, 1),
-                     "lookup_ceiling_Gproducts_per_s": round(ceiling, 1) if ceiling else None,
-                     "encode_frac_of_lookup_ceiling": round(enc_products / (ms_e / 1e3) / 1e9 / ceiling, 3)
-                     if ceiling else None,
-                     "reconstruct_frac_of_lookup_ceiling": round(dec_products / (ms_r / 1e3) / 1e9 / ceiling, 3)
-                     if ceiling else None,
+                     "lookups_per_product": {"encode": round(lk_e, 3), "reconstruct": round(lk_d, 3)},
+                     "lookup_ceiling_Gproducts_per_s": {"encode": round(ceil_e, 1), "reconstruct": round(ceil_d, 1)}
+                     if ceil_e else None,
+                     "encode_frac_of_lookup_ceiling": round(enc_products / (ms_e / 1e3) / 1e9 / ceil_e, 3)
+                     if ceil_e else None,
+                     "reconstruct_frac_of_lookup_ceiling": round(dec_products / (ms_r / 1e3) / 1e9 / ceil_d, 3)
+                     if ceil_d else None,
                      "bit_exact": bit_exact,
                      "cpu_baseline": {"encode_data_GBps": round(ce, 3), "reconstruct_data_GBps": round(cr, 3),
                                       "cores": threads, "kind": "port",
