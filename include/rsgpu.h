@@ -383,6 +383,12 @@ int rsgpu_xornet_available(void);
 /* Waits for queued background compiles; returns how many XOR-network
  * kernels are compiled in this process. */
 int rsgpu_xornet_sync(void);
+/* Drops queued background compiles and waits (at most 30 s) for the ones
+ * running; later launches of those matrices use the table kernels.  Call
+ * before exiting a process that may still be compiling: NVRTC registers
+ * exit handlers during its first compile, and they can run while that
+ * compile is still in progress.  The Python package calls it at exit. */
+int rsgpu_xornet_drain(void);
 /* Compiles now the XOR-network kernels a classic encoder's Encode and Verify
  * launch (every input / output tile), so their first calls run the network
  * rather than a table kernel.  Needs no device.  Returns the number of

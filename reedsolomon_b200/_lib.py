@@ -3,6 +3,7 @@
 The library is built in-tree by reedsolomon_b200.build; importing this module
 never falls back to anything else: a missing or unloadable library raises.
 """
+import atexit
 import ctypes
 import os
 
@@ -116,6 +117,7 @@ SIGNATURES = {
     "rsgpu_record_variant": (c_int, [c_int, c_int, c_size, c_int, c_int]),
     "rsgpu_xornet_available": (c_int, []),
     "rsgpu_xornet_sync": (c_int, []),
+    "rsgpu_xornet_drain": (c_int, []),
     "rsgpu_encoder_prepare_kernels": (c_int, [c_voidp]),
     "rsgpu_xornet_source": (ctypes.c_longlong, [c_voidp, c_int, c_int, c_int, c_int, c_int, ctypes.c_char_p,
                                                 c_size]),
@@ -169,6 +171,10 @@ def lib():
                 f.restype = res
                 f.argtypes = args
         _lib = L
+        # Background XOR-network compiles must not run into process teardown
+        # (NVRTC's own exit handlers can run while one is in progress):
+        # Python's atexit runs before any C-level exit handler.
+        atexit.register(L.rsgpu_xornet_drain)
     return _lib
 
 

@@ -925,6 +925,11 @@ int rsgpu_xornet_available(void) { return xornet_available() ? 1 : 0; }
 
 int rsgpu_xornet_sync(void) { return xornet_wait_idle(); }
 
+int rsgpu_xornet_drain(void) {
+    xornet_drain();
+    return RS_OK;
+}
+
 int rsgpu_encoder_prepare_kernels(rsgpu_encoder *enc) {
     if (!enc) return RS_ERR_INVALID_INPUT;
     if (enc->codec != RS_CODEC_CLASSIC || enc->p == 0 || !xornet_available()) return 0;

@@ -616,6 +616,11 @@ void worker_loop() {
             c.busy++;
         }
         std::vector<char> bin = build_kernel(job.first);
+        // NVRTC registers exit handlers of its own during its first compile
+        // (function-local statics); handlers run in reverse order, so the
+        // drain is registered once more after that, to run before them.
+        static std::once_flag after_first;
+        std::call_once(after_first, [] { std::atexit(drain_at_exit); });
         {
             std::lock_guard<std::mutex> lk(c.mu);
             job.second->cubin = std::move(bin);
@@ -626,10 +631,14 @@ void worker_loop() {
     }
 }
 
-// At exit (atexit, registered when the first worker starts; and again at
-// library unload) queued compiles are dropped and a compile in progress is
-// waited for (bounded), so no worker is inside NVRTC while the process
-// tears down.
+// At exit (atexit, registered when the first worker starts and again after
+// the first compile; and at library unload) queued compiles are dropped and
+// a compile in progress is waited for (bounded), so no worker is inside
+// NVRTC while the process tears down.  A compile that is still in NVRTC's
+// first run when exit starts can meet handlers NVRTC registered during that
+// run, which run first; hosts that may exit with compiles in flight call
+// rsgpu_xornet_drain() before exiting (the Python package does, through
+// atexit, which runs before any of the C-level teardown).
 void drain_at_exit() {
     Cache &c = cache();
     std::unique_lock<std::mutex> lk(c.mu);
@@ -786,6 +795,8 @@ struct XnArgs {
 bool xornet_available() { return nvrtc().ok; }
 
 int xornet_compile_count() { return g_compiles.load(); }
+
+void xornet_drain() { drain_at_exit(); }
 
 bool xornet_prepare(const GfMatArgs &a, int mode) {
     return a.n_in <= 32 && a.n_out <= kXornetMaxOut && lookup(a, mode, true) != nullptr;

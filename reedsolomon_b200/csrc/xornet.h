@@ -30,6 +30,8 @@ bool xornet_prepare(const GfMatArgs &a, int mode);
 int xornet_compile_count();
 // Waits for queued background compiles; returns the number of compiled kernels.
 int xornet_wait_idle();
+// Drops queued background compiles and waits (bounded) for those running.
+void xornet_drain();
 // Runs the XOR-network kernel over the whole 1 KiB chunks of a (16-byte
 // aligned shards only).  *bytes_done is 0 when it did not run: no NVRTC, an
 // unaligned pointer, a tile too large, or (sync == false) a matrix whose

@@ -8,6 +8,7 @@ import ctypes
 import os
 import shutil
 import subprocess
+import sys
 
 import pytest
 
@@ -72,8 +73,39 @@ def test_exit_with_compiles_in_flight(tmp_path):
                         "-I", CUDA_INC, os.path.join(HERE, "xornet_exit_queued.cpp"), "-o", str(exe),
                         "-L", PKG, "-lrsgpu", "-Wl,-rpath," + PKG, "-lpthread"], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-3000:]
-    for _ in range(3):
-        r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
+    for args in ([], [], [], ["warm"], ["warm"], ["warm"]):
+        r = subprocess.run([str(exe)] + args, capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0 and "queued" in r.stdout, (args, r.returncode, r.stderr[-2000:])
+
+
+_PY_EXIT = """
+import ctypes, sys, time
+sys.path.insert(0, {root!r})
+import reedsolomon_b200 as rs
+rs.lib()
+ctypes.CDLL({shim!r}).queue_compiles(0, 3)
+time.sleep(0.05)
+print("queued")
+"""
+
+
+@pytest.mark.skipif(shutil.which("g++") is None or not os.path.isdir(CUDA_INC) or not _nvrtc(),
+                    reason="needs g++, CUDA headers and libnvrtc")
+def test_python_exit_with_compiles_in_flight(tmp_path):
+    """A Python process that exits while its first background compiles run
+    exits cleanly: the package drains them through atexit, before NVRTC's
+    exit handlers (registered during its first compile) run.  Without that
+    drain this exited with SIGSEGV in about half of the runs."""
+    rs.lib()
+    shim = tmp_path / "libexitshim.so"
+    r = subprocess.run(["g++", "-std=c++17", "-O1", "-fPIC", "-shared", "-DRSGPU_EXIT_SHIM",
+                        "-I", os.path.join(PKG, "csrc"), "-I", os.path.join(ROOT, "include"), "-I", CUDA_INC,
+                        os.path.join(HERE, "xornet_exit_queued.cpp"), "-o", str(shim),
+                        "-L", PKG, "-lrsgpu", "-Wl,-rpath," + PKG], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
+    code = _PY_EXIT.format(root=ROOT, shim=str(shim))
+    for _ in range(8):
+        r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
         assert r.returncode == 0 and "queued" in r.stdout, (r.returncode, r.stderr[-2000:])
 
 
