@@ -205,11 +205,14 @@ def run_reference(args):
 
 def run_e2e(args, enc, lib, shards, S, stream, dev, world, barrier):
     """Encode through the host-buffer C-ABI entry point; every step moves the
-    data shards H2D from pinned memory and the parity D2H."""
+    data shards H2D from pinned memory and the parity D2H.  The host shards
+    are consecutive pieces of one pinned block, as the reference's Split
+    (reedsolomon.go:1803) and AllocAligned (unsafe.go:19-43) lay them out."""
     import torch
     import reedsolomon_b200 as rs
     k, p = K_DATA, P_PARITY
-    hs = [torch.empty(S, dtype=torch.uint8, pin_memory=True) for _ in range(k + p)]
+    block = torch.empty((k + p) * S, dtype=torch.uint8, pin_memory=True)
+    hs = [block[i * S:(i + 1) * S] for i in range(k + p)]
     for i in range(k):
         hs[i].copy_(shards[i])
     hptrs = rs._lib.ptr_array([h.data_ptr() for h in hs])

@@ -18,22 +18,22 @@ constexpr int kRing = 3;
 
 struct Pipeline {
     rsgpu_ctx *ctx;
-    size_t chunk = 0;
-    int rows = 0;  // staged rows per buffer
+    size_t chunk = 0;  // largest column chunk (the staging ring's row size)
+    int rows = 0;      // staged rows per buffer
     cudaEvent_t in_done[kRing], comp_done[kRing], out_done[kRing];
 
     int init(int n_rows, size_t size, size_t align) {
         rows = n_rows;
-        // ~8 chunks per call, at least 1 MiB per row, aligned for Leopard;
-        // with many rows (Leopard: up to 65536) the ring is held to 1 GiB.
-        size_t c = std::max<size_t>(size / 8, (size_t)1 << 20);
+        // ~4 full chunks per call (the tail is cut smaller, see chunks()), at
+        // least 1 MiB per row, aligned for Leopard; with many rows (Leopard:
+        // up to 65536) the ring is held to 1 GiB.
+        size_t c = std::max<size_t>(size / 4, (size_t)1 << 20);
         const size_t budget = ((size_t)1 << 30) / ((size_t)rows * kRing);
         c = std::min(c, std::max(budget, align));
         c = std::min(c, size);
         c = (c + align - 1) / align * align;
         chunk = std::min(c, size);
-        const size_t pitch = (chunk + 255) & ~(size_t)255;
-        int rc = ctx->staging.ensure(pitch * (size_t)rows * kRing);
+        int rc = ctx->staging.ensure(pitch() * (size_t)rows * kRing);
         if (rc) return rc;
         while (ctx->events.size() < 3 * kRing) {
             cudaEvent_t ev;
@@ -47,11 +47,44 @@ struct Pipeline {
         }
         return RS_OK;
     }
-    uint8_t *row(int b, int r) const {
-        const size_t pitch = (chunk + 255) & ~(size_t)255;
-        return ctx->staging.ptr + pitch * ((size_t)b * rows + r);
+    size_t pitch() const { return (chunk + 255) & ~(size_t)255; }
+    uint8_t *row(int b, int r) const { return ctx->staging.ptr + pitch() * ((size_t)b * rows + r); }
+    // Column chunks (offset, length): full chunks while at least two remain,
+    // then halves down to 1 MiB, so the last chunk, whose compute and D2H
+    // copies nothing overlaps, is small.  Every length but the last is a
+    // multiple of align.
+    std::vector<std::pair<size_t, size_t>> chunks(size_t size, size_t align) const {
+        std::vector<std::pair<size_t, size_t>> v;
+        const size_t tail_min = std::max<size_t>((size_t)1 << 20, align);
+        size_t off = 0;
+        while (off < size) {
+            const size_t rem = size - off;
+            size_t len = chunk;
+            if (rem < 2 * chunk) {
+                len = rem <= tail_min ? rem : std::max(tail_min, (rem / 2 + align - 1) / align * align);
+                len = std::min(len, std::min(chunk, rem));
+            }
+            v.emplace_back(off, len);
+            off += len;
+        }
+        return v;
     }
 };
+
+// Host rows idx[0..n) that are consecutive staging rows and sit at one
+// stride in host memory (the layout of Split's shards or of one allocation
+// cut into shards, unsafe.go:19-43) move with one 2D copy per chunk;
+// returns that stride, or 0.  A constant stride between separate
+// allocations is possible too; the driver rejects a 2D copy whose span
+// crosses them (invalid value), and run_pipeline then copies row by row.
+size_t host_stride(const std::vector<uint8_t *> &host_rows, const std::vector<int> &idx, size_t size) {
+    if (idx.size() < 2) return 0;
+    const ptrdiff_t st = host_rows[idx[1]] - host_rows[idx[0]];
+    if (st <= 0 || (size_t)st < size) return 0;
+    for (size_t j = 1; j < idx.size(); j++)
+        if (idx[j] != idx[0] + (int)j || host_rows[idx[j]] - host_rows[idx[j - 1]] != st) return 0;
+    return (size_t)st;
+}
 
 // Runs `compute(dev_rows, len)` over column chunks.  in_rows are copied
 // host->device before compute, out_rows device->host after it.  Row r of a
@@ -62,14 +95,31 @@ int run_pipeline(rsgpu_ctx *ctx, const std::vector<uint8_t *> &host_rows, const 
     Pipeline pl{ctx};
     int rc = pl.init((int)host_rows.size(), size, align);
     if (rc) return rc;
+    size_t in_stride = host_stride(host_rows, in_rows, size);
+    size_t out_stride = host_stride(host_rows, out_rows, size);
+    // A rejected 2D copy (span across allocations) clears its error state
+    // and turns the 2D path off for the rest of the call.
+    auto try_2d = [](cudaError_t e, size_t &stride) -> cudaError_t {
+        if (e == cudaErrorInvalidValue) {
+            cudaGetLastError();
+            stride = 0;
+            return cudaSuccess;
+        }
+        return e;
+    };
     std::vector<uint8_t *> dev(host_rows.size());
     int c = 0;
-    for (size_t off = 0; off < size; off += pl.chunk, c++) {
-        const size_t len = std::min(pl.chunk, size - off);
+    for (const auto &ch : pl.chunks(size, align)) {
+        const size_t off = ch.first, len = ch.second;
         const int b = c % kRing;
         if (c >= kRing) RS_CUDA(cudaStreamWaitEvent(ctx->copy_in, pl.out_done[b], 0));
-        for (int r : in_rows)
-            RS_CUDA(cudaMemcpyAsync(pl.row(b, r), host_rows[r] + off, len, cudaMemcpyHostToDevice, ctx->copy_in));
+        if (in_stride)
+            RS_CUDA(try_2d(cudaMemcpy2DAsync(pl.row(b, in_rows[0]), pl.pitch(), host_rows[in_rows[0]] + off,
+                                             in_stride, len, in_rows.size(), cudaMemcpyHostToDevice, ctx->copy_in),
+                           in_stride));
+        if (!in_stride)
+            for (int r : in_rows)
+                RS_CUDA(cudaMemcpyAsync(pl.row(b, r), host_rows[r] + off, len, cudaMemcpyHostToDevice, ctx->copy_in));
         RS_CUDA(cudaEventRecord(pl.in_done[b], ctx->copy_in));
         RS_CUDA(cudaStreamWaitEvent(ctx->stream, pl.in_done[b], 0));
         for (size_t r = 0; r < host_rows.size(); r++) dev[r] = pl.row(b, (int)r);
@@ -77,9 +127,15 @@ int run_pipeline(rsgpu_ctx *ctx, const std::vector<uint8_t *> &host_rows, const 
         if (rc) return rc;
         RS_CUDA(cudaEventRecord(pl.comp_done[b], ctx->stream));
         RS_CUDA(cudaStreamWaitEvent(ctx->copy_out, pl.comp_done[b], 0));
-        for (int r : out_rows)
-            RS_CUDA(cudaMemcpyAsync(host_rows[r] + off, pl.row(b, r), len, cudaMemcpyDeviceToHost, ctx->copy_out));
+        if (out_stride)
+            RS_CUDA(try_2d(cudaMemcpy2DAsync(host_rows[out_rows[0]] + off, out_stride, pl.row(b, out_rows[0]),
+                                             pl.pitch(), len, out_rows.size(), cudaMemcpyDeviceToHost, ctx->copy_out),
+                           out_stride));
+        if (!out_stride)
+            for (int r : out_rows)
+                RS_CUDA(cudaMemcpyAsync(host_rows[r] + off, pl.row(b, r), len, cudaMemcpyDeviceToHost, ctx->copy_out));
         RS_CUDA(cudaEventRecord(pl.out_done[b], ctx->copy_out));
+        c++;
     }
     RS_CUDA(cudaStreamSynchronize(ctx->copy_out));
     RS_CUDA(cudaStreamSynchronize(ctx->stream));

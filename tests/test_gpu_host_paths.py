@@ -161,3 +161,34 @@ def test_host_entry_points_refuse_mixed_and_leopard_progressive():
     leo = rs.New(k, p, rs.WithLeopardGF16())
     pa = L.ptr_array([hostt(a).data_ptr() for a in ref[k:]])
     assert lib.rsgpu_encode_idx_host(leo._h, hostt(ref[0]).data_ptr(), 0, pa, size) == -7
+
+
+@pytest.mark.parametrize("layout", ["block_pinned", "block_pageable", "separate_pinned"])
+@pytest.mark.parametrize("k,p,size", [(10, 4, (9 << 20) + 48), (4, 2, 1000)])
+def test_encode_and_reconstruct_host_layouts(layout, k, p, size):
+    """Host shards that are consecutive pieces of one block (one 2D copy per
+    pipeline chunk and direction) or separate allocations (per-row copies,
+    or a rejected 2D copy falling back to them), with full chunks, the
+    halving tail chunks and a ragged end: the parity and rebuilt shards
+    equal the oracle's."""
+    rng = np.random.default_rng(size + k)
+    ref = encoded(rng, k, p, size)
+    if layout.startswith("block"):
+        block = torch.zeros((k + p) * size, dtype=torch.uint8)
+        if layout == "block_pinned":
+            block = block.pin_memory()
+        sh = [block[i * size:(i + 1) * size] for i in range(k + p)]
+    else:
+        sh = [torch.zeros(size, dtype=torch.uint8).pin_memory() for _ in range(k + p)]
+    for i in range(k):
+        sh[i].copy_(torch.from_numpy(ref[i]))
+    enc = rs.New(k, p)
+    enc.Encode(sh)
+    for i in range(k, k + p):
+        assert np.array_equal(sh[i].numpy(), ref[i]), (layout, i)
+    # the lost shards are data shards 0..p-1: the survivors the decode reads
+    # are the consecutive rows p..k+p-1 (the rebuilt shards are new tensors)
+    work = [None if i < p else sh[i] for i in range(k + p)]
+    enc.Reconstruct(work)
+    for i in range(p):
+        assert np.array_equal(work[i].numpy(), ref[i]), (layout, i)
