@@ -313,8 +313,10 @@ def extra_reconstruct(enc, lib, shards, S, stream, cpu_seconds=3.0):
                 out[key]["hbm_frac_at_p50"] = round((k + 4) * S / (p50 / 1e3) / 1e9 / peaks()[0], 4)
     out["bit_exact"] = bit_exact
     assert bit_exact, "a reconstructed shard differs from the original bytes"
-    # end to end: host buffers, one pattern per call (rotating)
-    hs = [torch.empty(S, dtype=torch.uint8, pin_memory=True) for _ in range(k + p)]
+    # end to end: host buffers (consecutive pieces of one pinned block, like
+    # Split's shards), one pattern per call (rotating)
+    hblock = torch.empty((k + p) * S, dtype=torch.uint8, pin_memory=True)
+    hs = [hblock[i * S:(i + 1) * S] for i in range(k + p)]
     for i in range(k + p):
         hs[i].copy_(orig[i])
     hptrs = rs._lib.ptr_array([h.data_ptr() for h in hs])
@@ -332,7 +334,7 @@ def extra_reconstruct(enc, lib, shards, S, stream, cpu_seconds=3.0):
     e2e_ms = _pct(lat, 50)
     out["e2e_host_buffers"] = {"latency_ms_p50": round(e2e_ms, 3), "data_GBps_at_p50": round(k * S / (e2e_ms / 1e3) / 1e9, 2),
                                "h2d_bytes": k * S, "d2h_bytes": 4 * S, "path": "rsgpu_reconstruct_host, pinned"}
-    del hs
+    del hs, hblock
     # CPU: the reference's reconstruct kernel work (decode rows x first k present) on the host cores
     import oracle as O
     lost = combos[0]

@@ -71,19 +71,59 @@ struct Pipeline {
     }
 };
 
-// Host rows idx[0..n) that are consecutive staging rows and sit at one
-// stride in host memory (the layout of Split's shards or of one allocation
-// cut into shards, unsafe.go:19-43) move with one 2D copy per chunk;
-// returns that stride, or 0.  A constant stride between separate
-// allocations is possible too; the driver rejects a 2D copy whose span
-// crosses them (invalid value), and run_pipeline then copies row by row.
-size_t host_stride(const std::vector<uint8_t *> &host_rows, const std::vector<int> &idx, size_t size) {
-    if (idx.size() < 2) return 0;
-    const ptrdiff_t st = host_rows[idx[1]] - host_rows[idx[0]];
-    if (st <= 0 || (size_t)st < size) return 0;
-    for (size_t j = 1; j < idx.size(); j++)
-        if (idx[j] != idx[0] + (int)j || host_rows[idx[j]] - host_rows[idx[j - 1]] != st) return 0;
-    return (size_t)st;
+// Rows of one copy direction, as runs: consecutive staging rows (indices)
+// that sit at one stride in host memory (the layout of Split's shards or of
+// one allocation cut into shards, unsafe.go:19-43) move with one 2D copy per
+// chunk; a run of one row (stride 0) with a plain copy.  A constant stride
+// between separate allocations is possible too; the driver rejects a 2D copy
+// whose span crosses them (invalid value), and that run is then copied row
+// by row.
+struct Run {
+    int first, count;  // staging rows first .. first+count-1
+    size_t stride;     // host bytes between them, 0: one row at a time
+};
+
+std::vector<Run> make_runs(const std::vector<uint8_t *> &host_rows, const std::vector<int> &idx, size_t size) {
+    std::vector<Run> runs;
+    for (size_t j = 0; j < idx.size();) {
+        Run r{idx[j], 1, 0};
+        if (j + 1 < idx.size() && idx[j + 1] == idx[j] + 1) {
+            const ptrdiff_t st = host_rows[idx[j + 1]] - host_rows[idx[j]];
+            if (st > 0 && (size_t)st >= size) {
+                r.stride = (size_t)st;
+                while (j + r.count < idx.size() && idx[j + r.count] == idx[j] + r.count &&
+                       host_rows[idx[j + r.count]] - host_rows[idx[j + r.count - 1]] == st)
+                    r.count++;
+            }
+        }
+        runs.push_back(r);
+        j += r.count;
+    }
+    return runs;
+}
+
+// Copies column [off, off + len) of every row of the runs, host to staging
+// buffer b (h2d) or back, on stream st.
+int copy_runs(const Pipeline &pl, std::vector<Run> &runs, const std::vector<uint8_t *> &host_rows, int b,
+              size_t off, size_t len, bool h2d, cudaStream_t st) {
+    for (Run &r : runs) {
+        if (r.stride) {
+            cudaError_t e =
+                h2d ? cudaMemcpy2DAsync(pl.row(b, r.first), pl.pitch(), host_rows[r.first] + off, r.stride, len,
+                                        r.count, cudaMemcpyHostToDevice, st)
+                    : cudaMemcpy2DAsync(host_rows[r.first] + off, r.stride, pl.row(b, r.first), pl.pitch(), len,
+                                        r.count, cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) continue;
+            if (e != cudaErrorInvalidValue) RS_CUDA(e);
+            cudaGetLastError();  // rejected span: row copies from now on
+            r.stride = 0;
+        }
+        for (int q = r.first; q < r.first + r.count; q++) {
+            if (h2d) RS_CUDA(cudaMemcpyAsync(pl.row(b, q), host_rows[q] + off, len, cudaMemcpyHostToDevice, st));
+            else RS_CUDA(cudaMemcpyAsync(host_rows[q] + off, pl.row(b, q), len, cudaMemcpyDeviceToHost, st));
+        }
+    }
+    return RS_OK;
 }
 
 // Runs `compute(dev_rows, len)` over column chunks.  in_rows are copied
@@ -95,31 +135,15 @@ int run_pipeline(rsgpu_ctx *ctx, const std::vector<uint8_t *> &host_rows, const 
     Pipeline pl{ctx};
     int rc = pl.init((int)host_rows.size(), size, align);
     if (rc) return rc;
-    size_t in_stride = host_stride(host_rows, in_rows, size);
-    size_t out_stride = host_stride(host_rows, out_rows, size);
-    // A rejected 2D copy (span across allocations) clears its error state
-    // and turns the 2D path off for the rest of the call.
-    auto try_2d = [](cudaError_t e, size_t &stride) -> cudaError_t {
-        if (e == cudaErrorInvalidValue) {
-            cudaGetLastError();
-            stride = 0;
-            return cudaSuccess;
-        }
-        return e;
-    };
+    std::vector<Run> in_runs = make_runs(host_rows, in_rows, size), out_runs = make_runs(host_rows, out_rows, size);
     std::vector<uint8_t *> dev(host_rows.size());
     int c = 0;
     for (const auto &ch : pl.chunks(size, align)) {
         const size_t off = ch.first, len = ch.second;
         const int b = c % kRing;
         if (c >= kRing) RS_CUDA(cudaStreamWaitEvent(ctx->copy_in, pl.out_done[b], 0));
-        if (in_stride)
-            RS_CUDA(try_2d(cudaMemcpy2DAsync(pl.row(b, in_rows[0]), pl.pitch(), host_rows[in_rows[0]] + off,
-                                             in_stride, len, in_rows.size(), cudaMemcpyHostToDevice, ctx->copy_in),
-                           in_stride));
-        if (!in_stride)
-            for (int r : in_rows)
-                RS_CUDA(cudaMemcpyAsync(pl.row(b, r), host_rows[r] + off, len, cudaMemcpyHostToDevice, ctx->copy_in));
+        rc = copy_runs(pl, in_runs, host_rows, b, off, len, true, ctx->copy_in);
+        if (rc) return rc;
         RS_CUDA(cudaEventRecord(pl.in_done[b], ctx->copy_in));
         RS_CUDA(cudaStreamWaitEvent(ctx->stream, pl.in_done[b], 0));
         for (size_t r = 0; r < host_rows.size(); r++) dev[r] = pl.row(b, (int)r);
@@ -127,13 +151,8 @@ int run_pipeline(rsgpu_ctx *ctx, const std::vector<uint8_t *> &host_rows, const 
         if (rc) return rc;
         RS_CUDA(cudaEventRecord(pl.comp_done[b], ctx->stream));
         RS_CUDA(cudaStreamWaitEvent(ctx->copy_out, pl.comp_done[b], 0));
-        if (out_stride)
-            RS_CUDA(try_2d(cudaMemcpy2DAsync(host_rows[out_rows[0]] + off, out_stride, pl.row(b, out_rows[0]),
-                                             pl.pitch(), len, out_rows.size(), cudaMemcpyDeviceToHost, ctx->copy_out),
-                           out_stride));
-        if (!out_stride)
-            for (int r : out_rows)
-                RS_CUDA(cudaMemcpyAsync(host_rows[r] + off, pl.row(b, r), len, cudaMemcpyDeviceToHost, ctx->copy_out));
+        rc = copy_runs(pl, out_runs, host_rows, b, off, len, false, ctx->copy_out);
+        if (rc) return rc;
         RS_CUDA(cudaEventRecord(pl.out_done[b], ctx->copy_out));
         c++;
     }

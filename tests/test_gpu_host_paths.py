@@ -186,9 +186,11 @@ def test_encode_and_reconstruct_host_layouts(layout, k, p, size):
     enc.Encode(sh)
     for i in range(k, k + p):
         assert np.array_equal(sh[i].numpy(), ref[i]), (layout, i)
-    # the lost shards are data shards 0..p-1: the survivors the decode reads
-    # are the consecutive rows p..k+p-1 (the rebuilt shards are new tensors)
-    work = [None if i < p else sh[i] for i in range(k + p)]
-    enc.Reconstruct(work)
-    for i in range(p):
-        assert np.array_equal(work[i].numpy(), ref[i]), (layout, i)
+    # lost data shards 0..p-1: the survivors the decode reads are the
+    # consecutive rows p..k+p-1, one run (the rebuilt shards are new tensors);
+    # then scattered erasures: several runs of survivors
+    for lost in (list(range(p)), sorted(rng.choice(k + p, size=p, replace=False).tolist())):
+        work = [None if i in lost else sh[i] for i in range(k + p)]
+        enc.Reconstruct(work)
+        for i in lost:
+            assert np.array_equal(work[i].numpy(), ref[i]), (layout, lost, i)
