@@ -781,7 +781,9 @@ def extra_c1(dev, reps=200):
 
     rec_lat = lat(rec)
     rec_ok = all(torch.equal(sh[i], keep[j]) for j, i in enumerate(lost))
-    hs = [torch.empty(S, dtype=torch.uint8, pin_memory=True) for _ in range(k + p)]
+    # host shards: consecutive pieces of one pinned block, like Split's
+    hblock = torch.empty((k + p) * S, dtype=torch.uint8, pin_memory=True)
+    hs = [hblock[i * S:(i + 1) * S] for i in range(k + p)]
     for i in range(k):
         hs[i].copy_(sh[i])
     hptrs = rs._lib.ptr_array([h.data_ptr() for h in hs])

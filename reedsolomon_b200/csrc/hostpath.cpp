@@ -15,6 +15,12 @@ namespace rsgpu {
 namespace {
 
 constexpr int kRing = 3;
+// Smallest column chunk per row: 256 KiB when the rows move as 2D runs (a
+// 1 MiB shard still splits into four, so its copies in, compute and copies
+// out overlap), up to 1 MiB when they move one row per copy (a copy's fixed
+// cost, a few microseconds, must stay small against its bytes).
+constexpr size_t kMinChunk = (size_t)256 << 10;
+constexpr size_t kMinCopyBytes = (size_t)1 << 20;
 
 struct Pipeline {
     rsgpu_ctx *ctx;
@@ -22,12 +28,18 @@ struct Pipeline {
     int rows = 0;      // staged rows per buffer
     cudaEvent_t in_done[kRing], comp_done[kRing], out_done[kRing];
 
-    int init(int n_rows, size_t size, size_t align) {
+    size_t min_chunk = kMinChunk;
+
+    // rows_per_copy: the fewest rows one copy moves on average, in either
+    // direction (1 for row-by-row copies).
+    int init(int n_rows, size_t size, size_t align, double rows_per_copy) {
         rows = n_rows;
+        min_chunk = std::min(kMinCopyBytes,
+                             std::max(kMinChunk, (size_t)((double)kMinCopyBytes / std::max(1.0, rows_per_copy))));
         // ~4 full chunks per call (the tail is cut smaller, see chunks()), at
-        // least 1 MiB per row, aligned for Leopard; with many rows (Leopard:
-        // up to 65536) the ring is held to 1 GiB.
-        size_t c = std::max<size_t>(size / 4, (size_t)1 << 20);
+        // least min_chunk per row, aligned for Leopard; with many rows
+        // (Leopard: up to 65536) the ring is held to 1 GiB.
+        size_t c = std::max<size_t>(size / 4, min_chunk);
         const size_t budget = ((size_t)1 << 30) / ((size_t)rows * kRing);
         c = std::min(c, std::max(budget, align));
         c = std::min(c, size);
@@ -50,12 +62,12 @@ struct Pipeline {
     size_t pitch() const { return (chunk + 255) & ~(size_t)255; }
     uint8_t *row(int b, int r) const { return ctx->staging.ptr + pitch() * ((size_t)b * rows + r); }
     // Column chunks (offset, length): full chunks while at least two remain,
-    // then halves down to 1 MiB, so the last chunk, whose compute and D2H
+    // then halves down to min_chunk, so the last chunk, whose compute and D2H
     // copies nothing overlaps, is small.  Every length but the last is a
     // multiple of align.
     std::vector<std::pair<size_t, size_t>> chunks(size_t size, size_t align) const {
         std::vector<std::pair<size_t, size_t>> v;
-        const size_t tail_min = std::max<size_t>((size_t)1 << 20, align);
+        const size_t tail_min = std::max<size_t>(min_chunk, align);
         size_t off = 0;
         while (off < size) {
             const size_t rem = size - off;
@@ -83,7 +95,14 @@ struct Run {
     size_t stride;     // host bytes between them, 0: one row at a time
 };
 
-std::vector<Run> make_runs(const std::vector<uint8_t *> &host_rows, const std::vector<int> &idx, size_t size) {
+bool rejected(const rsgpu_ctx *ctx, const uint8_t *first, size_t stride, int count) {
+    for (const auto &t : ctx->rejected_2d)
+        if (std::get<0>(t) == first && std::get<1>(t) == stride && std::get<2>(t) == count) return true;
+    return false;
+}
+
+std::vector<Run> make_runs(const rsgpu_ctx *ctx, const std::vector<uint8_t *> &host_rows,
+                           const std::vector<int> &idx, size_t size) {
     std::vector<Run> runs;
     for (size_t j = 0; j < idx.size();) {
         Run r{idx[j], 1, 0};
@@ -94,6 +113,11 @@ std::vector<Run> make_runs(const std::vector<uint8_t *> &host_rows, const std::v
                 while (j + r.count < idx.size() && idx[j + r.count] == idx[j] + r.count &&
                        host_rows[idx[j + r.count]] - host_rows[idx[j + r.count - 1]] == st)
                     r.count++;
+                if (rejected(ctx, host_rows[r.first], r.stride, r.count)) {
+                    for (int q = 0; q < r.count; q++) runs.push_back(Run{r.first + q, 1, 0});
+                    j += r.count;
+                    continue;
+                }
             }
         }
         runs.push_back(r);
@@ -106,6 +130,7 @@ std::vector<Run> make_runs(const std::vector<uint8_t *> &host_rows, const std::v
 // buffer b (h2d) or back, on stream st.
 int copy_runs(const Pipeline &pl, std::vector<Run> &runs, const std::vector<uint8_t *> &host_rows, int b,
               size_t off, size_t len, bool h2d, cudaStream_t st) {
+    rsgpu_ctx *ctx = pl.ctx;
     for (Run &r : runs) {
         if (r.stride) {
             cudaError_t e =
@@ -116,6 +141,8 @@ int copy_runs(const Pipeline &pl, std::vector<Run> &runs, const std::vector<uint
             if (e == cudaSuccess) continue;
             if (e != cudaErrorInvalidValue) RS_CUDA(e);
             cudaGetLastError();  // rejected span: row copies from now on
+            if (ctx->rejected_2d.size() >= 64) ctx->rejected_2d.erase(ctx->rejected_2d.begin());
+            ctx->rejected_2d.emplace_back(host_rows[r.first], r.stride, r.count);
             r.stride = 0;
         }
         for (int q = r.first; q < r.first + r.count; q++) {
@@ -132,10 +159,15 @@ int copy_runs(const Pipeline &pl, std::vector<Run> &runs, const std::vector<uint
 template <class F>
 int run_pipeline(rsgpu_ctx *ctx, const std::vector<uint8_t *> &host_rows, const std::vector<int> &in_rows,
                  const std::vector<int> &out_rows, size_t size, size_t align, F compute) {
+    std::vector<Run> in_runs = make_runs(ctx, host_rows, in_rows, size),
+                     out_runs = make_runs(ctx, host_rows, out_rows, size);
+    auto per_copy = [](const std::vector<int> &idx, const std::vector<Run> &runs) {
+        return runs.empty() ? 1e9 : (double)idx.size() / (double)runs.size();
+    };
     Pipeline pl{ctx};
-    int rc = pl.init((int)host_rows.size(), size, align);
+    int rc = pl.init((int)host_rows.size(), size, align,
+                     std::min(per_copy(in_rows, in_runs), per_copy(out_rows, out_runs)));
     if (rc) return rc;
-    std::vector<Run> in_runs = make_runs(host_rows, in_rows, size), out_runs = make_runs(host_rows, out_rows, size);
     std::vector<uint8_t *> dev(host_rows.size());
     int c = 0;
     for (const auto &ch : pl.chunks(size, align)) {

@@ -6,6 +6,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/rsgpu.h"
@@ -48,6 +49,9 @@ struct rsgpu_ctx {
     rsgpu::DeviceBuffer scratch;  // verify temporaries, leopard work rows
     rsgpu::DeviceBuffer staging;  // host-path device copies of shards
     std::vector<cudaEvent_t> events;
+    // Host row layouts (first row, stride, rows) whose 2D copy the driver
+    // rejected (rows of separate allocations): copied row by row from then on.
+    std::vector<std::tuple<const uint8_t *, size_t, int>> rejected_2d;
     std::shared_ptr<rsgpu::LeoState> leo;  // Leopard tables, built on first use
     cudaMemPool_t pool = nullptr;  // stream-ordered scratch (keeps its memory, never trims)
 };
