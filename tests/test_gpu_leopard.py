@@ -26,8 +26,12 @@ def new(gf, k, p):
     return rs.New(k, p, rs.WithLeopardGF16() if gf == 16 else rs.WithLeopardGF())
 
 
+# GF(2^16) block sizes m = 1 .. 512: the encode's staged tables are compact
+# (no nibble tables for slots = 3 mod 4) for m = 2^even and full for
+# m = 2^odd, whose FFT has a distance-2 pass (m = 8, 32, 128, 512 here)
 CASES = [(16, 1, 1, 64), (16, 3, 2, 128), (16, 5, 3, 192), (16, 20, 13, 256), (16, 64, 64, 128),
-         (16, 300, 60, 128), (16, 500, 300, 64), (16, 10, 4, 4096),
+         (16, 300, 60, 128), (16, 500, 300, 64), (16, 10, 4, 4096), (16, 30, 7, 192), (16, 200, 100, 128),
+         (16, 100, 16, 64), (16, 70, 20, 128),
          (8, 1, 1, 64), (8, 5, 3, 128), (8, 40, 24, 256), (8, 100, 28, 64), (8, 192, 56, 128)]
 
 
