@@ -39,26 +39,39 @@ struct MulArgs {
     uint32_t m[8];
 };
 
+// Inputs are read in groups of kGrp 16-byte vectors, the next group's loads
+// issued before the current group's products (software pipelining: a
+// thread's HBM loads otherwise wait one latency per group, and with tiles
+// of a few KiB a thread has only one or two vectors per tile to overlap
+// them with).  Four inputs per group up to four outputs, two with 5-8
+// outputs, whose 32 accumulators leave fewer registers.
 template <int G>
 __device__ void batch_tile(const BatchJob &j, uint32_t tab_s, const Mul &mu, long long v0, long long v1,
                            uint32_t &mism) {
+    constexpr int kGrp = G == 1 ? 4 : 2;
+    const int n_in = j.n_in;
     for (long long v = v0 + threadIdx.x; v < v1; v += blockDim.x) {
         uint32_t acc[G][16];
 #pragma unroll
         for (int g = 0; g < G; g++)
 #pragma unroll
             for (int b = 0; b < 16; b++) acc[g][b] = 0;
-        int i = 0;
-        for (; i + 4 <= j.n_in; i += 4) {
-            const uint4 x0 = ld_in(j.in[i], v), x1 = ld_in(j.in[i + 1], v);
-            const uint4 x2 = ld_in(j.in[i + 2], v), x3 = ld_in(j.in[i + 3], v);
-            const uint32_t b = tab_s + i * kInStride;
-            mac_vec<G, kVariantPrmt>(x0, b, mu, acc);
-            mac_vec<G, kVariantPrmt>(x1, b + kInStride, mu, acc);
-            mac_vec<G, kVariantPrmt>(x2, b + 2 * kInStride, mu, acc);
-            mac_vec<G, kVariantPrmt>(x3, b + 3 * kInStride, mu, acc);
+        uint4 cur[kGrp], nxt[kGrp];
+#pragma unroll
+        for (int u = 0; u < kGrp; u++) {
+            cur[u] = u < n_in ? ld_in(j.in[u], v) : make_uint4(0, 0, 0, 0);
+            nxt[u] = make_uint4(0, 0, 0, 0);
         }
-        for (; i < j.n_in; i++) mac_vec<G, kVariantPrmt>(ld_in(j.in[i], v), tab_s + i * kInStride, mu, acc);
+        for (int i = 0; i < n_in; i += kGrp) {
+#pragma unroll
+            for (int u = 0; u < kGrp; u++)
+                if (i + kGrp + u < n_in) nxt[u] = ld_in(j.in[i + kGrp + u], v);
+#pragma unroll
+            for (int u = 0; u < kGrp; u++)
+                if (i + u < n_in) mac_vec<G, kVariantPrmt>(cur[u], tab_s + (i + u) * kInStride, mu, acc);
+#pragma unroll
+            for (int u = 0; u < kGrp; u++) cur[u] = nxt[u];
+        }
 #pragma unroll
         for (int g = 0; g < G; g++) {
             uint4 w[4];
@@ -86,7 +99,7 @@ __device__ void batch_tile(const BatchJob &j, uint32_t tab_s, const Mul &mu, lon
     }
 }
 
-__global__ void __launch_bounds__(kThreads) gf8_batch_kernel(const BatchJob *__restrict__ jobs, int njobs,
+__global__ void __launch_bounds__(kThreads, 4) gf8_batch_kernel(const BatchJob *__restrict__ jobs, int njobs,
                                                              const long long *__restrict__ cta_first,
                                                              int tile_vecs, int *flags, MulArgs mul) {
     extern __shared__ __align__(128) uint32_t smem_raw[];
