@@ -6,9 +6,10 @@
 // stripe operation becomes one GF(2^8) contraction job (<= 32 inputs, <= 8
 // outputs per job; more outputs become several jobs), the jobs' byte ranges
 // are cut into equal tiles, and ONE persistent launch processes all tiles:
-// CTA b owns a contiguous tile range whose cost ((inputs + outputs) x bytes)
-// is 1/grid of the total, so consecutive tiles mostly share a job and its
-// shared-memory product tables, and the SMs finish together.
+// CTA b owns a contiguous tile range whose cost (the larger of its
+// shared-memory lookups and its HBM bytes) is 1/grid of the total, so
+// consecutive tiles mostly share a job and its shared-memory product tables,
+// and the SMs finish together.
 #include <algorithm>
 #include <atomic>
 #include <climits>
@@ -250,7 +251,7 @@ int add_jobs(rsgpu_batch *b, const uint8_t *rows, int n_in, int n_out, const std
     return RS_OK;
 }
 
-// Cost-balanced contiguous tile ranges, one per CTA.
+// Cost-balanced contiguous tile ranges, one per CTA (cost: see job_cost).
 void plan_tiles(rsgpu_batch *b, std::vector<long long> &cta_first) {
     const int tile = b->tile_bytes > 0 ? b->tile_bytes : kDefaultTile;
     long long t = 0;
@@ -263,9 +264,14 @@ void plan_tiles(rsgpu_batch *b, std::vector<long long> &cta_first) {
         const long long nt = (j.nbytes + tile - 1) / tile;
         t += nt;
         const int rw = j.n_in + j.n_out * (j.mode == kModeWrite ? 1 : 2);
-        job_cost[i] = (double)rw * (double)j.nbytes;
+        // Time per byte column: the larger of the shared-memory lookups
+        // (two per input byte and output group of four, 32 per clock per SM)
+        // and the HBM bytes (about 22 per clock per SM at the measured copy
+        // rate), in units of one group's lookups per input byte.
+        const int groups = (j.n_out + 3) / 4;
+        job_cost[i] = std::max((double)j.n_in * groups, 0.72 * rw) * (double)j.nbytes;
         total += job_cost[i];
-        b->bytes += job_cost[i];
+        b->bytes += (double)rw * (double)j.nbytes;
     }
     b->n_tiles = t;
     // resident CTAs per SM of the batch kernel, queried once per device
