@@ -100,60 +100,68 @@ __device__ void batch_tile(const BatchJob &j, uint32_t tab_s, const Mul &mu, lon
     }
 }
 
+// Work is handed out dynamically: the tile list is cut into cost-balanced
+// units of consecutive tiles (kUnitsPerCta per CTA on average), and each CTA
+// takes the next unit from a global counter until none is left, so CTAs
+// that drew slower tiles take fewer units.  unit_first[u] is unit u's first
+// tile, unit_job[u] the job holding it; a CTA's units come in increasing
+// order, and it rebuilds its tables only when a unit starts another job.
 __global__ void __launch_bounds__(kThreads, 4) gf8_batch_kernel(const BatchJob *__restrict__ jobs, int njobs,
-                                                             const long long *__restrict__ cta_first,
-                                                             int tile_vecs, int *flags, MulArgs mul) {
+                                                             const long long *__restrict__ unit_first,
+                                                             const int *__restrict__ unit_job, int n_units,
+                                                             int *counter, int tile_vecs, int *flags, MulArgs mul) {
     extern __shared__ __align__(128) uint32_t smem_raw[];
     __shared__ BatchJob sj;
-    __shared__ int s_job;
+    __shared__ int s_job, s_unit;
     __shared__ long long s_next;
     uint32_t *tab = aligned_tables(smem_raw);
     const uint32_t tab_s = (uint32_t)__cvta_generic_to_shared(tab);
-    const long long t0 = cta_first[blockIdx.x], t1 = cta_first[blockIdx.x + 1];
     Mul mu;
 #pragma unroll
     for (int j = 0; j < 8; j++) mu.m[j] = mul.m[j];
     int job = -1;
     long long next_begin = 0;
     uint32_t mism = 0;
-    for (long long t = t0; t < t1; t++) {
-        if (job < 0 || t >= next_begin) {
-            __syncthreads();  // previous job's tables are no longer read
-            if (threadIdx.x == 0) {
-                int j = job;
-                if (j < 0) {  // first job of this CTA: binary search on tile_begin
-                    int lo = 0, hi = njobs - 1;
-                    while (lo < hi) {
-                        const int mid = (lo + hi + 1) >> 1;
-                        if (jobs[mid].tile_begin <= t) lo = mid;
-                        else hi = mid - 1;
-                    }
-                    j = lo;
-                } else {
+    for (;;) {
+        __syncthreads();  // every thread has read s_unit (and s_job) of the previous unit
+        if (threadIdx.x == 0) s_unit = atomicAdd(counter, 1);
+        __syncthreads();
+        const int u = s_unit;
+        if (u >= n_units) break;
+        const long long t0 = unit_first[u], t1 = unit_first[u + 1];
+        for (long long t = t0; t < t1; t++) {
+            if (job < 0 || t >= next_begin || t < sj.tile_begin) {
+                __syncthreads();  // previous job's tables are no longer read
+                if (threadIdx.x == 0) {
+                    int j = job;
+                    if (t == t0) j = unit_job[u];  // first tile of a unit
                     while (j + 1 < njobs && jobs[j + 1].tile_begin <= t) j++;
+                    s_job = j;
+                    s_next = (j + 1 < njobs) ? jobs[j + 1].tile_begin : LLONG_MAX;
                 }
-                s_job = j;
-                s_next = (j + 1 < njobs) ? jobs[j + 1].tile_begin : LLONG_MAX;
+                __syncthreads();
+                const int nj = s_job;
+                next_begin = s_next;
+                if (nj != job) {
+                    if (mism && job >= 0 && sj.flag >= 0) flags[sj.flag] = 1;
+                    mism = 0;
+                    job = nj;
+                    __syncthreads();
+                    const uint32_t *src = reinterpret_cast<const uint32_t *>(jobs + job);
+                    uint32_t *dst = reinterpret_cast<uint32_t *>(&sj);
+                    for (int w = threadIdx.x; w < (int)(sizeof(BatchJob) / 4); w += blockDim.x) dst[w] = src[w];
+                    __syncthreads();
+                    if (sj.n_out <= 4) build_tables_from<1>(tab, sj.coef, sj.n_in, sj.n_out);
+                    else build_tables_from<2>(tab, sj.coef, sj.n_in, sj.n_out);
+                    __syncthreads();
+                }
             }
-            __syncthreads();
-            if (mism && job >= 0 && sj.flag >= 0) flags[sj.flag] = 1;
-            mism = 0;
-            job = s_job;
-            next_begin = s_next;
-            __syncthreads();
-            const uint32_t *src = reinterpret_cast<const uint32_t *>(jobs + job);
-            uint32_t *dst = reinterpret_cast<uint32_t *>(&sj);
-            for (int w = threadIdx.x; w < (int)(sizeof(BatchJob) / 4); w += blockDim.x) dst[w] = src[w];
-            __syncthreads();
-            if (sj.n_out <= 4) build_tables_from<1>(tab, sj.coef, sj.n_in, sj.n_out);
-            else build_tables_from<2>(tab, sj.coef, sj.n_in, sj.n_out);
-            __syncthreads();
+            const long long nvec = sj.nbytes >> 4;
+            const long long v0 = (t - sj.tile_begin) * tile_vecs;
+            const long long v1 = v0 + tile_vecs < nvec ? v0 + tile_vecs : nvec;
+            if (sj.n_out <= 4) batch_tile<1>(sj, tab_s, mu, v0, v1, mism);
+            else batch_tile<2>(sj, tab_s, mu, v0, v1, mism);
         }
-        const long long nvec = sj.nbytes >> 4;
-        const long long v0 = (t - sj.tile_begin) * tile_vecs;
-        const long long v1 = v0 + tile_vecs < nvec ? v0 + tile_vecs : nvec;
-        if (sj.n_out <= 4) batch_tile<1>(sj, tab_s, mu, v0, v1, mism);
-        else batch_tile<2>(sj, tab_s, mu, v0, v1, mism);
     }
     if (mism && job >= 0 && sj.flag >= 0) flags[sj.flag] = 1;
 }
@@ -178,8 +186,11 @@ struct rsgpu_batch {
     // device state
     BatchJob *d_jobs = nullptr;
     size_t d_jobs_cap = 0;
-    long long *d_cta = nullptr;
+    long long *d_cta = nullptr;  // first tile of every work unit
     size_t d_cta_cap = 0;
+    int *d_ujob = nullptr;  // job of every unit's first tile
+    size_t d_ujob_cap = 0;
+    int n_units = 0;
     int *d_flags = nullptr;
     size_t d_flags_cap = 0;
     int grid = 0;
@@ -191,6 +202,7 @@ struct rsgpu_batch {
         if (graph) cudaGraphExecDestroy(graph);
         cudaFree(d_jobs);
         cudaFree(d_cta);
+        cudaFree(d_ujob);
         cudaFree(d_flags);
     }
 };
@@ -199,6 +211,7 @@ namespace {
 
 constexpr int kDefaultTile = 16384;
 constexpr int kBatchBlocksPerSm = 4;
+constexpr int kUnitsPerCta = 8;  // work units per persistent CTA, on average
 
 int get_encoder(rsgpu_batch *b, int k, int p, rsgpu_encoder **out) {
     auto key = std::make_pair(k, p);
@@ -251,8 +264,11 @@ int add_jobs(rsgpu_batch *b, const uint8_t *rows, int n_in, int n_out, const std
     return RS_OK;
 }
 
-// Cost-balanced contiguous tile ranges, one per CTA (cost: see job_cost).
-void plan_tiles(rsgpu_batch *b, std::vector<long long> &cta_first) {
+// Cost-balanced units of consecutive tiles (cost: see job_cost), about
+// kUnitsPerCta per CTA, handed out at run time (gf8_batch_kernel);
+// unit_first has n_units + 1 entries, unit_job the job of each unit's
+// first tile.
+void plan_tiles(rsgpu_batch *b, std::vector<long long> &unit_first, std::vector<int> &unit_job) {
     const int tile = b->tile_bytes > 0 ? b->tile_bytes : kDefaultTile;
     long long t = 0;
     double total = 0;
@@ -288,22 +304,30 @@ void plan_tiles(rsgpu_batch *b, std::vector<long long> &cta_first) {
     const int per_sm = std::min(resident, b->ctas_per_sm > 0 ? b->ctas_per_sm : kBatchBlocksPerSm);
     const int grid = std::max(1, (int)std::min<long long>(t, (long long)b->ctx->info.sm_count * per_sm));
     b->grid = grid;
-    cta_first.assign(grid + 1, t);
-    cta_first[0] = 0;
-    // walk jobs, handing out tiles until each CTA's share of cost is reached
+    const int n_units = (int)std::max(1LL, std::min<long long>(t, (long long)grid * kUnitsPerCta));
+    b->n_units = n_units;
+    unit_first.assign(n_units + 1, t);
+    unit_first[0] = 0;
+    // walk jobs, handing out tiles until each unit's share of cost is reached
     double acc = 0;
-    int cta = 1;
-    for (size_t i = 0; i < b->jobs.size() && cta < grid; i++) {
+    int unit = 1;
+    for (size_t i = 0; i < b->jobs.size() && unit < n_units; i++) {
         const BatchJob &j = b->jobs[i];
         const long long nt = (j.nbytes + tile - 1) / tile;
         const double per_tile = job_cost[i] / (double)nt;
-        for (long long k = 0; k < nt && cta < grid; k++) {
+        for (long long k = 0; k < nt && unit < n_units; k++) {
             acc += per_tile;
-            while (cta < grid && acc >= total * cta / grid) cta_first[cta++] = j.tile_begin + k + 1;
+            while (unit < n_units && acc >= total * unit / n_units) unit_first[unit++] = j.tile_begin + k + 1;
         }
     }
-    for (int c = 1; c <= grid; c++) cta_first[c] = std::max(cta_first[c], cta_first[c - 1]);
-    cta_first[grid] = t;
+    for (int u = 1; u <= n_units; u++) unit_first[u] = std::max(unit_first[u], unit_first[u - 1]);
+    unit_first[n_units] = t;
+    unit_job.assign(n_units, 0);
+    size_t jj = 0;
+    for (int u = 0; u < n_units; u++) {
+        while (jj + 1 < b->jobs.size() && b->jobs[jj + 1].tile_begin <= unit_first[u]) jj++;
+        unit_job[u] = (int)jj;
+    }
 }
 
 // Uploads the job table and CTA ranges, stream-ordered on `st`: growing a
@@ -312,8 +336,9 @@ void plan_tiles(rsgpu_batch *b, std::vector<long long> &cta_first) {
 // server can plan one slot's micro-batch while other streams keep running.
 int upload(rsgpu_batch *b, cudaStream_t st) {
     if (!b->dirty) return RS_OK;
-    std::vector<long long> cta_first;
-    plan_tiles(b, cta_first);
+    std::vector<long long> unit_first;
+    std::vector<int> unit_job;
+    plan_tiles(b, unit_first, unit_job);
     cudaMemPool_t pool = b->ctx->pool;
     auto grow = [st, pool](auto *&ptr, size_t &cap, size_t want) -> cudaError_t {
         if (want <= cap) return cudaSuccess;
@@ -329,13 +354,16 @@ int upload(rsgpu_batch *b, cudaStream_t st) {
         return e;
     };
     RS_CUDA(grow(b->d_jobs, b->d_jobs_cap, std::max<size_t>(1, b->jobs.size()) * sizeof(BatchJob)));
-    RS_CUDA(grow(b->d_cta, b->d_cta_cap, cta_first.size() * sizeof(long long)));
-    RS_CUDA(grow(b->d_flags, b->d_flags_cap, std::max(1, b->n_stripes) * sizeof(int)));
+    RS_CUDA(grow(b->d_cta, b->d_cta_cap, unit_first.size() * sizeof(long long)));
+    RS_CUDA(grow(b->d_ujob, b->d_ujob_cap, unit_job.size() * sizeof(int)));
+    // the stripes' flags, then the unit counter of the persistent launch
+    RS_CUDA(grow(b->d_flags, b->d_flags_cap, (std::max(1, b->n_stripes) + 1) * sizeof(int)));
     if (!b->jobs.empty())
         RS_CUDA(cudaMemcpyAsync(b->d_jobs, b->jobs.data(), b->jobs.size() * sizeof(BatchJob), cudaMemcpyHostToDevice,
                                 st));
-    RS_CUDA(cudaMemcpyAsync(b->d_cta, cta_first.data(), cta_first.size() * sizeof(long long), cudaMemcpyHostToDevice,
-                            st));
+    RS_CUDA(cudaMemcpyAsync(b->d_cta, unit_first.data(), unit_first.size() * sizeof(long long),
+                            cudaMemcpyHostToDevice, st));
+    RS_CUDA(cudaMemcpyAsync(b->d_ujob, unit_job.data(), unit_job.size() * sizeof(int), cudaMemcpyHostToDevice, st));
     if (b->graph) {
         cudaGraphExecDestroy(b->graph);
         b->graph = nullptr;
@@ -350,8 +378,9 @@ int launch_persistent(rsgpu_batch *b, cudaStream_t st) {
     const size_t smem = (size_t)kMaxIn * kInStride + kTableAlign;
     MulArgs mul;
     for (int i = 0; i < 8; i++) mul.m[i] = kMulInit[i];
-    gf8_batch_kernel<<<b->grid, kThreads, smem, st>>>(b->d_jobs, (int)b->jobs.size(), b->d_cta, tile / 16,
-                                                     b->d_flags, mul);
+    int *counter = b->d_flags + std::max(1, b->n_stripes);  // zeroed with the flags before every run
+    gf8_batch_kernel<<<b->grid, kThreads, smem, st>>>(b->d_jobs, (int)b->jobs.size(), b->d_cta, b->d_ujob,
+                                                     b->n_units, counter, tile / 16, b->d_flags, mul);
     RS_CUDA(cudaGetLastError());
     return RS_OK;
 }
@@ -526,7 +555,8 @@ int rsgpu::batch_run_on(rsgpu_batch *b, int mode, cudaStream_t st) {
     rsgpu_ctx *ctx = b->ctx;
     int rc = upload(b, st);
     if (rc) return rc;
-    RS_CUDA(cudaMemsetAsync(b->d_flags, 0, std::max(1, b->n_stripes) * sizeof(int), st));
+    // the stripes' flags and the persistent launch's unit counter
+    RS_CUDA(cudaMemsetAsync(b->d_flags, 0, (std::max(1, b->n_stripes) + 1) * sizeof(int), st));
     if (mode == RS_BATCH_PERSISTENT) {
         rc = launch_persistent(b, st);
         if (rc) return rc;
