@@ -211,7 +211,7 @@ namespace {
 
 constexpr int kDefaultTile = 16384;
 constexpr int kBatchBlocksPerSm = 4;
-constexpr int kUnitsPerCta = 8;  // work units per persistent CTA, on average
+constexpr int kUnitsPerCta = 16;  // work units per persistent CTA, on average
 
 int get_encoder(rsgpu_batch *b, int k, int p, rsgpu_encoder **out) {
     auto key = std::make_pair(k, p);
