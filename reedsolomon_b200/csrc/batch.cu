@@ -5,11 +5,12 @@
 // idle for small stripes and pays launch latency per call.  Here every
 // stripe operation becomes one GF(2^8) contraction job (<= 32 inputs, <= 8
 // outputs per job; more outputs become several jobs), the jobs' byte ranges
-// are cut into equal tiles, and ONE persistent launch processes all tiles:
-// CTA b owns a contiguous tile range whose cost (the larger of its
-// shared-memory lookups and its HBM bytes) is 1/grid of the total, so
-// consecutive tiles mostly share a job and its shared-memory product tables,
-// and the SMs finish together.
+// are cut into equal tiles, and ONE persistent launch processes all tiles.
+// Consecutive tiles are grouped into units of equal cost (the larger of
+// their shared-memory lookups and their HBM bytes), which the CTAs take
+// from a global counter at run time: a CTA's consecutive tiles mostly share
+// a job and its shared-memory product tables, and CTAs that draw slower
+// tiles take fewer units, so the SMs finish together.
 #include <algorithm>
 #include <atomic>
 #include <climits>
