@@ -36,6 +36,7 @@ struct Pipeline {
         rows = n_rows;
         min_chunk = std::min(kMinCopyBytes,
                              std::max(kMinChunk, (size_t)((double)kMinCopyBytes / std::max(1.0, rows_per_copy))));
+        min_chunk = (min_chunk + align - 1) / align * align;  // every chunk but the last is a multiple of align
         // ~4 full chunks per call (the tail is cut smaller, see chunks()), at
         // least min_chunk per row, aligned for Leopard; with many rows
         // (Leopard: up to 65536) the ring is held to 1 GiB.

@@ -194,3 +194,27 @@ def test_encode_and_reconstruct_host_layouts(layout, k, p, size):
         enc.Reconstruct(work)
         for i in lost:
             assert np.array_equal(work[i].numpy(), ref[i]), (layout, lost, i)
+
+
+@pytest.mark.parametrize("leopard", [True, False])
+def test_host_chunks_stay_aligned_with_mixed_layouts(leopard):
+    """Host shards in runs of different lengths (data shards 0-1 in one block,
+    2 alone, the parity in another block: 1.5 rows per 2D copy) make the
+    pipeline's minimum chunk 1 MiB / 1.5, which must still be rounded to the
+    codec's alignment (64 bytes for Leopard) for every chunk but the last."""
+    k, p, size = 3, 2, 3 << 20
+    rng = np.random.default_rng(99 + leopard)
+    ref = [rng.integers(0, 256, size, dtype=np.uint8) for _ in range(k)] + [np.zeros(size, np.uint8) for _ in range(p)]
+    if leopard:
+        assert O.leo_encode(16, k, p, ref) == 0
+        enc = rs.New(k, p, rs.WithLeopardGF16())
+    else:
+        assert O.rs_encode(k, p, ref) == 0
+        enc = rs.New(k, p)
+    data01 = torch.from_numpy(np.concatenate(ref[:2])).pin_memory()
+    data2 = torch.from_numpy(ref[2].copy()).pin_memory()
+    par = torch.zeros(p * size, dtype=torch.uint8).pin_memory()
+    sh = [data01[:size], data01[size:], data2] + [par[j * size:(j + 1) * size] for j in range(p)]
+    enc.Encode(sh)
+    for j in range(p):
+        assert np.array_equal(sh[k + j].numpy(), ref[k + j]), (leopard, j)
