@@ -89,8 +89,8 @@ struct Pipeline {
 // one allocation cut into shards, unsafe.go:19-43) move with one 2D copy per
 // chunk; a run of one row (stride 0) with a plain copy.  A constant stride
 // between separate allocations is possible too; the driver rejects a 2D copy
-// whose span crosses them (invalid value), and that run is then copied row
-// by row.
+// whose span crosses them (invalid value) or whose stride exceeds its
+// largest pitch (invalid pitch), and that run is then copied row by row.
 struct Run {
     int first, count;  // staging rows first .. first+count-1
     size_t stride;     // host bytes between them, 0: one row at a time
@@ -140,8 +140,10 @@ int copy_runs(const Pipeline &pl, std::vector<Run> &runs, const std::vector<uint
                     : cudaMemcpy2DAsync(host_rows[r.first] + off, r.stride, pl.row(b, r.first), pl.pitch(), len,
                                         r.count, cudaMemcpyDeviceToHost, st);
             if (e == cudaSuccess) continue;
-            if (e != cudaErrorInvalidValue) RS_CUDA(e);
-            cudaGetLastError();  // rejected span: row copies from now on
+            // a span across allocations (invalid value) or a stride past the
+            // largest pitch a copy takes (invalid pitch): row copies from now on
+            if (e != cudaErrorInvalidValue && e != cudaErrorInvalidPitchValue) RS_CUDA(e);
+            cudaGetLastError();
             if (ctx->rejected_2d.size() >= 64) ctx->rejected_2d.erase(ctx->rejected_2d.begin());
             ctx->rejected_2d.emplace_back(host_rows[r.first], r.stride, r.count);
             r.stride = 0;
