@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cstring>
 
+#include "host_chunks.h"
 #include "rsgpu_internal.h"
 #include "trace.h"
 
@@ -15,37 +16,20 @@ namespace rsgpu {
 namespace {
 
 constexpr int kRing = 3;
-// Smallest column chunk per row: 256 KiB when the rows move as 2D runs (a
-// 1 MiB shard still splits into four, so its copies in, compute and copies
-// out overlap), up to 1 MiB when they move one row per copy (a copy's fixed
-// cost, a few microseconds, must stay small against its bytes).
-constexpr size_t kMinChunk = (size_t)256 << 10;
-constexpr size_t kMinCopyBytes = (size_t)1 << 20;
 
 struct Pipeline {
     rsgpu_ctx *ctx;
     size_t chunk = 0;  // largest column chunk (the staging ring's row size)
     int rows = 0;      // staged rows per buffer
     cudaEvent_t in_done[kRing], comp_done[kRing], out_done[kRing];
-
-    size_t min_chunk = kMinChunk;
+    HostChunkPlan plan;
 
     // rows_per_copy: the fewest rows one copy moves on average, in either
-    // direction (1 for row-by-row copies).
+    // direction (1 for row-by-row copies); the chunks: host_chunks.h.
     int init(int n_rows, size_t size, size_t align, double rows_per_copy) {
         rows = n_rows;
-        min_chunk = std::min(kMinCopyBytes,
-                             std::max(kMinChunk, (size_t)((double)kMinCopyBytes / std::max(1.0, rows_per_copy))));
-        min_chunk = (min_chunk + align - 1) / align * align;  // every chunk but the last is a multiple of align
-        // ~4 full chunks per call (the tail is cut smaller, see chunks()), at
-        // least min_chunk per row, aligned for Leopard; with many rows
-        // (Leopard: up to 65536) the ring is held to 1 GiB.
-        size_t c = std::max<size_t>(size / 4, min_chunk);
-        const size_t budget = ((size_t)1 << 30) / ((size_t)rows * kRing);
-        c = std::min(c, std::max(budget, align));
-        c = std::min(c, size);
-        c = (c + align - 1) / align * align;
-        chunk = std::min(c, size);
+        plan = plan_host_chunks(size, rows, kRing, align, rows_per_copy);
+        chunk = plan.chunk;
         int rc = ctx->staging.ensure(pitch() * (size_t)rows * kRing);
         if (rc) return rc;
         while (ctx->events.size() < 3 * kRing) {
@@ -62,26 +46,6 @@ struct Pipeline {
     }
     size_t pitch() const { return (chunk + 255) & ~(size_t)255; }
     uint8_t *row(int b, int r) const { return ctx->staging.ptr + pitch() * ((size_t)b * rows + r); }
-    // Column chunks (offset, length): full chunks while at least two remain,
-    // then halves down to min_chunk, so the last chunk, whose compute and D2H
-    // copies nothing overlaps, is small.  Every length but the last is a
-    // multiple of align.
-    std::vector<std::pair<size_t, size_t>> chunks(size_t size, size_t align) const {
-        std::vector<std::pair<size_t, size_t>> v;
-        const size_t tail_min = std::max<size_t>(min_chunk, align);
-        size_t off = 0;
-        while (off < size) {
-            const size_t rem = size - off;
-            size_t len = chunk;
-            if (rem < 2 * chunk) {
-                len = rem <= tail_min ? rem : std::max(tail_min, (rem / 2 + align - 1) / align * align);
-                len = std::min(len, std::min(chunk, rem));
-            }
-            v.emplace_back(off, len);
-            off += len;
-        }
-        return v;
-    }
 };
 
 // Rows of one copy direction, as runs: consecutive staging rows (indices)
@@ -173,7 +137,7 @@ int run_pipeline(rsgpu_ctx *ctx, const std::vector<uint8_t *> &host_rows, const 
     if (rc) return rc;
     std::vector<uint8_t *> dev(host_rows.size());
     int c = 0;
-    for (const auto &ch : pl.chunks(size, align)) {
+    for (const auto &ch : pl.plan.chunks) {
         const size_t off = ch.first, len = ch.second;
         const int b = c % kRing;
         if (c >= kRing) RS_CUDA(cudaStreamWaitEvent(ctx->copy_in, pl.out_done[b], 0));
