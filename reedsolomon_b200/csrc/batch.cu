@@ -17,6 +17,7 @@
 #include <cstring>
 #include <map>
 
+#include "batch_plan.h"
 #include "gf8_device.cuh"
 #include "rsgpu_internal.h"
 #include "trace.h"
@@ -265,14 +266,13 @@ int add_jobs(rsgpu_batch *b, const uint8_t *rows, int n_in, int n_out, const std
     return RS_OK;
 }
 
-// Cost-balanced units of consecutive tiles (cost: see job_cost), about
-// kUnitsPerCta per CTA, handed out at run time (gf8_batch_kernel);
-// unit_first has n_units + 1 entries, unit_job the job of each unit's
-// first tile.
+// Cost-balanced units of consecutive tiles (cost: see job_cost; the cut:
+// batch_plan.h), about kUnitsPerCta per CTA, handed out at run time
+// (gf8_batch_kernel); unit_first has n_units + 1 entries, unit_job the job
+// of each unit's first tile.
 void plan_tiles(rsgpu_batch *b, std::vector<long long> &unit_first, std::vector<int> &unit_job) {
     const int tile = b->tile_bytes > 0 ? b->tile_bytes : kDefaultTile;
     long long t = 0;
-    double total = 0;
     std::vector<double> job_cost(b->jobs.size());
     b->bytes = 0;
     for (size_t i = 0; i < b->jobs.size(); i++) {
@@ -287,7 +287,6 @@ void plan_tiles(rsgpu_batch *b, std::vector<long long> &unit_first, std::vector<
         // rate), in units of one group's lookups per input byte.
         const int groups = (j.n_out + 3) / 4;
         job_cost[i] = std::max((double)j.n_in * groups, 0.72 * rw) * (double)j.nbytes;
-        total += job_cost[i];
         b->bytes += (double)rw * (double)j.nbytes;
     }
     b->n_tiles = t;
@@ -307,28 +306,14 @@ void plan_tiles(rsgpu_batch *b, std::vector<long long> &unit_first, std::vector<
     b->grid = grid;
     const int n_units = (int)std::max(1LL, std::min<long long>(t, (long long)grid * kUnitsPerCta));
     b->n_units = n_units;
-    unit_first.assign(n_units + 1, t);
-    unit_first[0] = 0;
-    // walk jobs, handing out tiles until each unit's share of cost is reached
-    double acc = 0;
-    int unit = 1;
-    for (size_t i = 0; i < b->jobs.size() && unit < n_units; i++) {
-        const BatchJob &j = b->jobs[i];
-        const long long nt = (j.nbytes + tile - 1) / tile;
-        const double per_tile = job_cost[i] / (double)nt;
-        for (long long k = 0; k < nt && unit < n_units; k++) {
-            acc += per_tile;
-            while (unit < n_units && acc >= total * unit / n_units) unit_first[unit++] = j.tile_begin + k + 1;
-        }
+    std::vector<long long> begins(b->jobs.size()), counts(b->jobs.size());
+    for (size_t i = 0; i < b->jobs.size(); i++) {
+        begins[i] = b->jobs[i].tile_begin;
+        counts[i] = (b->jobs[i].nbytes + tile - 1) / tile;
     }
-    for (int u = 1; u <= n_units; u++) unit_first[u] = std::max(unit_first[u], unit_first[u - 1]);
-    unit_first[n_units] = t;
-    unit_job.assign(n_units, 0);
-    size_t jj = 0;
-    for (int u = 0; u < n_units; u++) {
-        while (jj + 1 < b->jobs.size() && b->jobs[jj + 1].tile_begin <= unit_first[u]) jj++;
-        unit_job[u] = (int)jj;
-    }
+    BatchUnitPlan plan = plan_batch_units(begins, counts, job_cost, n_units);
+    unit_first = std::move(plan.unit_first);
+    unit_job = std::move(plan.unit_job);
 }
 
 // Uploads the job table and CTA ranges, stream-ordered on `st`: growing a
