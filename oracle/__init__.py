@@ -38,6 +38,7 @@ _SIGS = {
                                    ctypes.POINTER(c_int), c_voidp]),
     "ora_leo16_tables": (None, [c_voidp] * 4),
     "ora_leo16_mullog": (ctypes.c_uint16, [ctypes.c_uint16, ctypes.c_uint16]),
+    "ora_leo_simd": (c_int, [c_int]),
     "ora_leo16_encode": (c_int, [c_int, c_int, c_voidp, c_size]),
     "ora_leo16_reconstruct": (c_int, [c_int, c_int, c_voidp, c_voidp, c_size, c_int, c_voidp]),
     "ora_leo16_errlocs": (c_int, [c_int, c_int, c_voidp, c_voidp]),
@@ -229,6 +230,13 @@ def leo8_tables():
     skew = np.zeros(255, np.uint8)
     lib().ora_leo8_tables(log.ctypes.data, exp.ctypes.data, skew.ctypes.data, walsh.ctypes.data)
     return log, exp, skew, walsh
+
+
+def leo_simd(on):
+    """CPU-baseline timing only: AVX2 nibble-table products in the Leopard
+    codec (True) or the scalar restatement (False, the checker's default).
+    Returns whether the AVX2 path is on."""
+    return bool(lib().ora_leo_simd(int(bool(on))))
 
 
 def leo_encode(gf, k, p, shards):

@@ -684,13 +684,114 @@ uint16_t ora_leo16_mullog(uint16_t a, uint16_t log_b) {
     return mullog16(a, log_b);
 }
 
+static void xor_into_avx2(uint8_t *out, const uint8_t *in, size_t n);
+static int leo_simd;
+
 static inline void xor_into(uint8_t *out, const uint8_t *in, size_t n) {
+#if defined(__x86_64__) || defined(__i386__)
+    if (leo_simd) {
+        xor_into_avx2(out, in, n);
+        return;
+    }
+#endif
     for (size_t i = 0; i < n; i++) out[i] ^= in[i];
 }
+
+/* CPU-baseline only (bench.py's Leopard CPU leg): AVX2 nibble-table
+ * multiplies, the approach of the reference's mulgf16 / mulgf8 AVX2 kernels
+ * (_gen/gf16.go, _gen/gf8.go: each input nibble selects a 16-entry table of
+ * the product's low and high output bytes with PSHUFB).  Off unless
+ * ora_leo_simd(1) is called; the checker's products stay the scalar
+ * refMulAdd / refMul restatements below, and a CPU test requires both to give
+ * the same bytes. */
+int ora_leo_simd(int on) {
+#if defined(__x86_64__) || defined(__i386__)
+    leo_simd = on && __builtin_cpu_supports("avx2");
+#else
+    leo_simd = 0;
+    (void)on;
+#endif
+    return leo_simd;
+}
+
+#if defined(__x86_64__) || defined(__i386__)
+#include <immintrin.h>
+/* out ^= in (sliceXor, galois_amd64.go:162-203, with AVX2) */
+__attribute__((target("avx2"))) static void xor_into_avx2(uint8_t *out, const uint8_t *in, size_t n) {
+    size_t i = 0;
+    for (; i + 32 <= n; i += 32)
+        _mm256_storeu_si256((__m256i *)(out + i), _mm256_xor_si256(_mm256_loadu_si256((const __m256i *)(out + i)),
+                                                                    _mm256_loadu_si256((const __m256i *)(in + i))));
+    for (; i < n; i++) out[i] ^= in[i];
+}
+/* x (^)= y*log_m over whole 64-byte chunks; t: the refMulAdd table of log_m.
+ * Nibble q of a symbol (bits 4q..4q+3) picks t[e], t[e << 4], t[256 + e] or
+ * t[256 + (e << 4)] for q = 0..3 (refMul's table is the XOR of two nibble
+ * tables per input byte). */
+__attribute__((target("avx2"))) static void muladd16_avx2(uint8_t *x, const uint8_t *y, const uint16_t *t,
+                                                          size_t n, int accumulate) {
+    uint8_t tb[8][16];
+    for (int e = 0; e < 16; e++) {
+        const uint16_t v[4] = {t[e], t[e << 4], t[256 + e], t[256 + (e << 4)]};
+        for (int q = 0; q < 4; q++) {
+            tb[2 * q][e] = (uint8_t)v[q];
+            tb[2 * q + 1][e] = (uint8_t)(v[q] >> 8);
+        }
+    }
+    __m256i T[8];
+    for (int i = 0; i < 8; i++) T[i] = _mm256_broadcastsi128_si256(_mm_loadu_si128((const __m128i *)tb[i]));
+    const __m256i m4 = _mm256_set1_epi8(0x0F);
+    for (size_t off = 0; off + 64 <= n; off += 64) {
+        const __m256i lo = _mm256_loadu_si256((const __m256i *)(y + off));
+        const __m256i hi = _mm256_loadu_si256((const __m256i *)(y + off + 32));
+        const __m256i n0 = _mm256_and_si256(lo, m4), n1 = _mm256_and_si256(_mm256_srli_epi64(lo, 4), m4);
+        const __m256i n2 = _mm256_and_si256(hi, m4), n3 = _mm256_and_si256(_mm256_srli_epi64(hi, 4), m4);
+        __m256i plo = _mm256_xor_si256(_mm256_xor_si256(_mm256_shuffle_epi8(T[0], n0), _mm256_shuffle_epi8(T[2], n1)),
+                                       _mm256_xor_si256(_mm256_shuffle_epi8(T[4], n2), _mm256_shuffle_epi8(T[6], n3)));
+        __m256i phi = _mm256_xor_si256(_mm256_xor_si256(_mm256_shuffle_epi8(T[1], n0), _mm256_shuffle_epi8(T[3], n1)),
+                                       _mm256_xor_si256(_mm256_shuffle_epi8(T[5], n2), _mm256_shuffle_epi8(T[7], n3)));
+        if (accumulate) {
+            plo = _mm256_xor_si256(plo, _mm256_loadu_si256((const __m256i *)(x + off)));
+            phi = _mm256_xor_si256(phi, _mm256_loadu_si256((const __m256i *)(x + off + 32)));
+        }
+        _mm256_storeu_si256((__m256i *)(x + off), plo);
+        _mm256_storeu_si256((__m256i *)(x + off + 32), phi);
+    }
+}
+
+/* x (^)= t[y] bytewise, t: a 256-entry GF(2^8) product table (linear, so
+ * t[y] = t[y & 15] ^ t[y & 0xF0]). */
+__attribute__((target("avx2"))) static void muladd8_avx2(uint8_t *x, const uint8_t *y, const uint8_t *t, size_t n,
+                                                         int accumulate) {
+    uint8_t tl[16], th[16];
+    for (int e = 0; e < 16; e++) {
+        tl[e] = t[e];
+        th[e] = t[e << 4];
+    }
+    const __m256i TL = _mm256_broadcastsi128_si256(_mm_loadu_si128((const __m128i *)tl));
+    const __m256i TH = _mm256_broadcastsi128_si256(_mm_loadu_si128((const __m128i *)th));
+    const __m256i m4 = _mm256_set1_epi8(0x0F);
+    size_t i = 0;
+    for (; i + 32 <= n; i += 32) {
+        const __m256i v = _mm256_loadu_si256((const __m256i *)(y + i));
+        __m256i r = _mm256_xor_si256(_mm256_shuffle_epi8(TL, _mm256_and_si256(v, m4)),
+                                     _mm256_shuffle_epi8(TH, _mm256_and_si256(_mm256_srli_epi64(v, 4), m4)));
+        if (accumulate) r = _mm256_xor_si256(r, _mm256_loadu_si256((const __m256i *)(x + i)));
+        _mm256_storeu_si256((__m256i *)(x + i), r);
+    }
+    for (; i < n; i++) x[i] = (uint8_t)((accumulate ? x[i] : 0) ^ t[y[i]]);
+}
+#endif
 
 /* leopard.go:907-925 refMulAdd: x ^= y*log_m on 64-byte chunks (32 lo | 32 hi) */
 static void muladd16(uint8_t *x, const uint8_t *y, uint16_t log_m, size_t n) {
     const uint16_t *t = lut16(log_m);
+#if defined(__x86_64__) || defined(__i386__)
+    if (leo_simd) {
+        muladd16_avx2(x, y, t, n, 1);
+        return;
+    }
+#endif
     for (size_t off = 0; off + 64 <= n; off += 64)
         for (int i = 0; i < 32; i++) {
             uint16_t prod = t[y[off + i]] ^ t[256 + y[off + 32 + i]];
@@ -701,6 +802,12 @@ static void muladd16(uint8_t *x, const uint8_t *y, uint16_t log_m, size_t n) {
 /* leopard.go:966-981 refMul: x = y*log_m */
 static void mul16(uint8_t *x, const uint8_t *y, uint16_t log_m, size_t n) {
     const uint16_t *t = lut16(log_m);
+#if defined(__x86_64__) || defined(__i386__)
+    if (leo_simd) {
+        muladd16_avx2(x, y, t, n, 0);
+        return;
+    }
+#endif
     for (size_t off = 0; off + 64 <= n; off += 64)
         for (int i = 0; i < 32; i++) {
             uint16_t prod = t[y[off + i]] ^ t[256 + y[off + 32 + i]];
@@ -1052,10 +1159,22 @@ uint64_t ora_leo8_gfni_matrix(uint8_t log_m) {
 /* leopard8.go:891-916 refMulAdd8 / refMul8 */
 static void muladd8(uint8_t *x, const uint8_t *y, uint8_t lm, size_t n) {
     const uint8_t *t = l8_lut[lm];
+#if defined(__x86_64__) || defined(__i386__)
+    if (leo_simd) {
+        muladd8_avx2(x, y, t, n, 1);
+        return;
+    }
+#endif
     for (size_t i = 0; i < n; i++) x[i] ^= t[y[i]];
 }
 static void mul8(uint8_t *x, const uint8_t *y, uint8_t lm, size_t n) {
     const uint8_t *t = l8_lut[lm];
+#if defined(__x86_64__) || defined(__i386__)
+    if (leo_simd) {
+        muladd8_avx2(x, y, t, n, 0);
+        return;
+    }
+#endif
     for (size_t i = 0; i < n; i++) x[i] = t[y[i]];
 }
 /* galois_noasm.go:101-105 fftDIT28, :115-119 ifftDIT28 */

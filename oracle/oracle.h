@@ -87,6 +87,10 @@ int ora_rs_decode_rows(int k, int p, int kind, const uint8_t *present, int data_
 void ora_leo16_tables(uint16_t *log_out, uint16_t *exp_out, uint16_t *skew_out,
                       uint16_t *walsh_out);
 uint16_t ora_leo16_mullog(uint16_t a, uint16_t log_b);
+/* CPU-baseline timing only: 1 switches the Leopard products to AVX2
+ * nibble-table multiplies (when the CPU has AVX2), 0 back to the scalar
+ * restatement; returns whether the AVX2 path is on. */
+int ora_leo_simd(int on);
 int ora_leo16_encode(int k, int p, uint8_t *const *shards, size_t size);
 int ora_leo16_reconstruct(int k, int p, uint8_t *const *shards, const uint8_t *present,
                           size_t size, int recover_all, uint8_t *written);
